@@ -1,0 +1,394 @@
+#!/usr/bin/env python3
+"""TABI-PB solve throughput on B200 -- prints one JSON line.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl gpu|reference]
+
+Workload (one "step" = one complete TABI-PB solve of one molecule):
+  synthetic globular molecule, 2,000 atoms uniform in an 18 A sphere (minimum
+  separation 2.0 A: 3 A is geometrically infeasible at that density), radii
+  U(1.5, 2.0) A, charges N(0, 0.4) e shifted to an integer net charge, seed 0;
+  surface from the project's MSMS-format generator at 10 vertices/A^2
+  (~98k faces after the reference's face filter); eps 1/80, 0.15 M; Taylor
+  order 3, MAC 0.8, leaf 500; GMRES tol 1e-4 (MAXL 10, NRMAX 10); FP64.
+  The step runs form_matrix -> tree -> interaction lists -> leaf-block LU ->
+  GMRES -> solvation energy on device-resident inputs (tabi_run_dev).
+
+`value` is solves/s over all ranks (device time, CUDA events, max over
+ranks); `e2e` runs the same solve through the host-array C ABI
+(tabi_form_matrix ... tabi_energy) with the host<->device copies inside the
+timed region.  Multi-GPU runs are independent replicas (one molecule per
+rank, weak scaling).  `--impl reference` times the CPU restatement of the
+reference (oracle/, all host threads) on a bounded sample of the same solve.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path[:0] = [os.path.join(ROOT, "tabi-pb_b200"), os.path.join(ROOT, "oracle")]
+
+WORKLOAD = dict(natm=2000, radius=18.0, min_sep=2.0, density=10.0, probe=1.4, seed=0,
+                order=3, theta=0.8, maxparnode=500, tol=1e-4, eps0=1.0, eps1=80.0, bulk=0.15)
+WORKLOAD_NAME = "globular-2000-atoms-18A-10vA2-p3-mac0.8-leaf500-fp64"
+METRIC = "solves/s (TABI-PB solve at <=1e-4 dG error; plain FP64)"
+# GMRES iterations of this workload, from the parity-checked GPU run (the
+# oracle reproduces the GPU's iteration count; used to scale the CPU sample)
+WORKLOAD_ITERS = None
+OPS_NEAR_PAIR = 64  # algorithmic ops per near-field pair (reference formulas)
+
+
+def far_ops(p):
+    from math import comb
+
+    return 2 * (47 * comb(p + 3, 3) + 12 * comb(p + 6, 3))
+
+
+def make_inputs():
+    import oracle as O
+    from tabipb import surface as S
+
+    w = WORKLOAD
+    xyz, q, r = S.synthetic_molecule(w["natm"], w["radius"], min_sep=w["min_sep"],
+                                     seed=w["seed"])
+    pos, nrm, fc, h = S.gaussian_surface(xyz, r, density=w["density"], probe=w["probe"])
+    fc, _ = O.surface_area(pos, fc)  # readin.f90:264-333 face filter
+    return dict(sptpos=np.ascontiguousarray(pos), sptnrm=np.ascontiguousarray(nrm),
+                nvert=np.ascontiguousarray(fc, dtype=np.int32),
+                chrpos=np.ascontiguousarray(xyz), atmchr=np.ascontiguousarray(q), grid=h)
+
+
+class Clocks:
+    """nvidia-smi sampler for the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index=0):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for name, v in zip(("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown",
+                                "sw_power_cap"), f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(name)
+        return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=smax,
+                    reasons=sorted(reasons), samples=len(sm))
+
+
+# ---------------------------------------------------------------- oracle sample
+def oracle_estimate(inp, iters, nthreads, target_sample=32768, leaf_sample=48,
+                    atom_sample=200, face_frac=0.5):
+    """Times the CPU restatement of the reference on a bounded sample of one
+    solve and extrapolates: form_matrix RHS on a face subset, full tree build,
+    one matvec (moments + a spread sample of targets), one preconditioner
+    apply (a few leaves, scaled by sum (2n)^3 -- the reference re-factors
+    every leaf on every apply), energy on an atom subset.
+    Solve = form + tree + iters*matvec + (iters+2)*msolve + energy."""
+    import oracle as O
+
+    w = WORKLOAD
+    kap = O.kappa(w["bulk"], w["eps1"])
+    eps = w["eps1"] / w["eps0"]
+    nface = len(inp["nvert"])
+    natm = len(inp["atmchr"])
+    t = {}
+    # form_matrix: geometry for all faces; RHS sum on a face subset
+    xyz, tq, ar, _ = O.form_matrix(inp["sptpos"], inp["sptnrm"], inp["nvert"], np.zeros((0, 3)),
+                                   np.zeros(0), w["eps0"])
+    sub = inp["nvert"][:: max(1, int(round(1.0 / face_frac)))]
+    t0 = time.perf_counter()
+    O.form_matrix(inp["sptpos"], inp["sptnrm"], sub, inp["chrpos"], inp["atmchr"], w["eps0"])
+    t["form"] = (time.perf_counter() - t0) * nface / len(sub)
+    t0 = time.perf_counter()
+    T = O.Tree(xyz, tq, ar, None, w["order"], w["maxparnode"], w["theta"])
+    t["tree"] = time.perf_counter() - t0
+    x = np.random.default_rng(0).normal(size=2 * nface)
+    t0 = time.perf_counter()
+    T.matvec_prepare(x)
+    t_prep = time.perf_counter() - t0
+    nb = 16
+    per = max(1, target_sample // nb)
+    starts = np.linspace(0, nface - per, nb).astype(int)
+    t0 = time.perf_counter()
+    for s0 in starts:
+        T.matvec_targets(kap, eps, s0, s0 + per, nthreads=nthreads)
+    t_s = time.perf_counter() - t0
+    t["matvec"] = t_prep + t_s * nface / (nb * per)
+    ib, nr = T.leaves()
+    order = np.argsort(nr)
+    pick = order[np.linspace(0, len(order) - 1, min(leaf_sample, len(order))).astype(int)]
+    r = np.random.default_rng(1).normal(size=2 * nface)
+    t0 = time.perf_counter()
+    if leaf_sample >= len(nr):
+        pick = order
+        T.msolve(kap, eps, r, iprcd=1, nthreads=nthreads)
+    else:
+        for lf in pick:
+            T.msolve(kap, eps, r, iprcd=1, leaf0=int(lf), leaf1=int(lf) + 1, nthreads=nthreads)
+    t_l = time.perf_counter() - t0
+    cube = (2.0 * nr.astype(float)) ** 3
+    t["msolve"] = t_l * cube.sum() / cube[pick].sum()
+    asub = np.arange(0, natm, max(1, natm // atom_sample))
+    t0 = time.perf_counter()
+    O.energy_surface(T.xyz, T.tq, T.area, inp["chrpos"][asub], inp["atmchr"][asub], kap, eps,
+                     w["eps0"], np.random.default_rng(2).normal(size=2 * nface),
+                     nthreads=nthreads)
+    t["energy"] = (time.perf_counter() - t0) * natm / len(asub)
+    solve = t["form"] + t["tree"] + iters * t["matvec"] + (iters + 2) * t["msolve"] + t["energy"]
+    sample = (f"form_matrix RHS on {len(sub)} of {nface} faces; full tree; one matvec = "
+              f"moments + {nb * per} of {nface} targets (16 spread blocks); one "
+              f"preconditioner apply = {len(pick)} of {len(nr)} leaves scaled by sum (2n)^3; "
+              f"energy on {len(asub)} of {natm} atoms; solve = form + tree + {iters} matvecs + "
+              f"{iters + 2} applies + energy")
+    return 1.0 / solve, t, sample
+
+
+# ---------------------------------------------------------------- GPU arm
+def gpu_arm(args):
+    import torch
+    import torch.distributed as dist
+
+    import tabipb
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    w = WORKLOAD
+    inp = make_inputs()
+    dev = torch.device("cuda", local)
+    d = {k: torch.from_numpy(inp[k]).to(dev) for k in ("sptpos", "sptnrm", "nvert", "chrpos",
+                                                       "atmchr")}
+    nspt, nface, natm = len(inp["sptpos"]), len(inp["nvert"]), len(inp["atmchr"])
+    kap = tabipb.kappa(w["bulk"], w["eps1"])
+    solver = tabipb.TabiSolver(order=w["order"], maxparnode=w["maxparnode"], theta=w["theta"],
+                               kappa=kap, eps0=w["eps0"], eps1=w["eps1"], tol=w["tol"])
+    stream = torch.cuda.current_stream(dev)
+    sp = stream.cuda_stream
+
+    def step():
+        return solver.run_dev(nspt, d["sptpos"].data_ptr(), d["sptnrm"].data_ptr(), nface,
+                              d["nvert"].data_ptr(), natm, d["chrpos"].data_ptr(),
+                              d["atmchr"].data_ptr(), None, sp)
+
+    fp64_peak = tabipb.probe_fp64_peak(300.0)
+    for _ in range(args.warmup):
+        res = step()
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    clocks.start()
+    solver.profile(True)
+    times = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        res = step()
+        e1.record(stream)
+        times.append((e0, e1))
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = sum(a.elapsed_time(b) for a, b in times)
+    prof = solver.profile_read()
+    solver.profile(False)
+    ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+
+    # ---- end to end through the host-array C ABI
+    e2e_steps = max(1, min(args.steps, 3))
+    h2d = 0
+    d2h = 0
+
+    def e2e_once():
+        nonlocal h2d, d2h
+        with tabipb.TabiSolver(order=w["order"], maxparnode=w["maxparnode"], theta=w["theta"],
+                               kappa=kap, eps0=w["eps0"], eps1=w["eps1"], tol=w["tol"]) as s:
+            xyz, tq, ar, b = s.form_matrix(inp["sptpos"], inp["sptnrm"], inp["nvert"],
+                                           inp["chrpos"], inp["atmchr"])
+            s.build_tree()
+            _, _, _, bt = s.permute(bvct=b)
+            r = s.dgmres(bt)
+            se, ce = s.energy(inp["chrpos"], inp["atmchr"], r["x"])
+        h2d = (inp["sptpos"].nbytes + inp["sptnrm"].nbytes + inp["nvert"].nbytes
+               + inp["chrpos"].nbytes + inp["atmchr"].nbytes + 2 * bt.nbytes
+               + inp["chrpos"].nbytes + inp["atmchr"].nbytes + r["x"].nbytes)
+        d2h = (xyz.nbytes + tq.nbytes + ar.nbytes + b.nbytes + 4 * nface + r["x"].nbytes + 16)
+        return se
+
+    e2e_once()  # warm-up
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(e2e_steps):
+        se_e2e = e2e_once()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_t = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_s = float(e2e_t.item())
+
+    out = None
+    if rank == 0:
+        near_ms, near_n = prof["near"]
+        far_ms, far_n = prof["far"]
+        mv_ms = sum(prof[k][0] for k in ("moments", "far", "near", "reduce"))
+        n_mv = max(near_n, 1)
+        near_pairs, far_int = res["near_pairs"], res["far"]
+        near_avg_s = near_ms / max(near_n, 1) / 1e3
+        achieved = near_pairs * OPS_NEAR_PAIR / near_avg_s / 1e12
+        peak = fp64_peak / 1e12
+        value = world * args.steps / (ms_max / 1e3)
+        out = {
+            "metric": METRIC,
+            "value": value,
+            "unit": "solves/s",
+            "n_gpus": world,
+            "steps": args.steps,
+            "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps,
+            "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": None,
+            "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": WORKLOAD_NAME, "faces": nface, "vertices": nspt,
+                       "atoms": natm, "order": w["order"], "theta": w["theta"],
+                       "maxparnode": w["maxparnode"], "tol": w["tol"],
+                       "gmres_iterations": res["iter"], "leaves": res["nleaf"],
+                       "soleng_kcal_mol": res["soleng"],
+                       "parallelism": f"replicas x{world}",
+                       "l2": "256 MB buffer written between timed steps"},
+            "matvec_interactions_per_s": (near_pairs + far_int) / (mv_ms / n_mv / 1e3),
+            "interactions_per_matvec": {"near_pairs": near_pairs, "far": far_int},
+            "phase_ms_per_step": {k: v[0] / args.steps for k, v in prof.items() if k != "all"},
+            "roofline": {"kernel": "near_kernel (COMPP_DIRECT_PB)", "bound": "fp64",
+                         "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "peak_source": "DFMA loop probe (tabi_probe_fp64_peak), this GPU",
+                         "ops_per_launch": near_pairs * OPS_NEAR_PAIR,
+                         "avg_launch_ms": near_avg_s * 1e3},
+            "e2e": {"value": world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": int(prof["all"][1]),
+            "clocks": clk,
+        }
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, parts, sample = oracle_estimate(inp, res["iter"], nthreads=1)
+        out["cpu_baseline"] = {"value": v, "unit": "solves/s", "cores": 1, "kind": "port",
+                               "sample": sample,
+                               "phase_s": {k: round(x, 4) for k, x in parts.items()}}
+    if out is not None:
+        print(json.dumps(out), flush=True)
+    solver.close()
+
+
+# ---------------------------------------------------------------- reference arm
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if rank != 0:
+        return
+    nthreads = os.cpu_count() or 1
+    inp = make_inputs()
+    iters = WORKLOAD_ITERS or args.iters
+    vals, parts, sample = [], None, ""
+    for _ in range(args.warmup):
+        oracle_estimate(inp, iters, nthreads, target_sample=2048, leaf_sample=4, atom_sample=16,
+                        face_frac=0.05)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        v, parts, sample = oracle_estimate(inp, iters, nthreads, target_sample=65536,
+                                           leaf_sample=10 ** 9, atom_sample=400)
+        vals.append(v)
+    wall = time.perf_counter() - t0
+    value = float(np.mean(vals))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD_NAME, "faces": len(inp["nvert"]),
+                   "atoms": len(inp["atmchr"]), "gmres_iterations": iters},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads,
+                         "kind": "port", "sample": sample,
+                         "phase_s": {k: round(x, 4) for k, x in parts.items()}},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+        "sample_wall_s": wall,
+    }), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("gpu", "reference"), default="gpu")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--iters", type=int, default=12,
+                    help="GMRES iterations used to scale the reference-arm sample")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

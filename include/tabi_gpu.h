@@ -1,0 +1,187 @@
+/*
+ * tabi_gpu.h -- C ABI of the B200 TABI-PB solve path (libtabi_gpu.so).
+ *
+ * The reference (gengwh/TABI-PB, Fortran) solves the boundary-integral
+ * Poisson-Boltzmann system with a treecode matvec, a leaf-block-diagonal
+ * preconditioner and SLATEC GMRES, all driven from module globals by
+ * src/main.f90.  Each entry point below replaces one reference interface; the
+ * citation is given with each.  A Fortran caller binds them with
+ * ISO_C_BINDING (interface blocks with bind(C), value arguments, c_double
+ * arrays); see INTEGRATION.md.
+ *
+ * Conventions
+ *  - All arrays are host arrays unless the name ends in _dev (device
+ *    pointers, with a cudaStream_t passed as void*; NULL = the handle's own
+ *    stream).
+ *  - Layouts are the reference's: coordinates are column-major 3 x N
+ *    (point i at [3i, 3i+2]); face vertex lists and orderarr are 1-based;
+ *    vectors of length 2N are [x1 ; x2] (potential ; normal derivative).
+ *  - After tabi_build_tree, every length-N / 2N vector exchanged with the
+ *    library is in TREE ORDER, exactly as the reference's bvct/xvct are after
+ *    treecode_initialization (main.f90:447-453).
+ *  - Every function returns 0 on success or a negative TABI_ERR_* code;
+ *    tabi_last_error() gives the message.  A handle is not thread-safe.
+ */
+#ifndef TABI_GPU_H
+#define TABI_GPU_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TABI_OK 0
+#define TABI_ERR_ARG (-1)       /* invalid argument */
+#define TABI_ERR_CUDA (-2)      /* CUDA runtime error */
+#define TABI_ERR_NOMEM (-3)     /* device or host allocation failed */
+#define TABI_ERR_STATE (-4)     /* call out of order (e.g. matvec before tree) */
+#define TABI_ERR_SINGULAR (-5)  /* a leaf block LU hit an exact zero pivot */
+#define TABI_ERR_LIMIT (-6)     /* an internal size limit was exceeded */
+
+#define TABI_PREC_FP64 0 /* plain FP64 treecode (the reference's arithmetic) */
+
+typedef struct tabi_handle_s* tabi_h;
+
+/* usrdata.in parameters (main.f90:39-50) and the hard-coded solver settings
+ * (main.f90:55-58, 93-97).  kappa is the inverse Debye length as main.f90:62-63
+ * computes it (see tabi_kappa).  theta must be in (0, 1): the reference's
+ * self-interaction removal (treecode3d_pb.f:1169-1172) relies on the MAC
+ * failing for every cluster that contains the target. */
+typedef struct {
+  int order;       /* Taylor order p (1..8) */
+  int maxparnode;  /* leaf size L */
+  double theta;    /* MAC */
+  double kappa;    /* 1/A */
+  double eps0;     /* interior dielectric (epsp) */
+  double eps1;     /* exterior dielectric (epsw) */
+  int iprcd;       /* 1 = leaf-block preconditioner, else diagonal scaling */
+  double tol;      /* GMRES tolerance (reference: 1e-4) */
+  int maxl;        /* GMRES restart length (reference: 10) */
+  int nrmax;       /* max restarts (reference: 10) */
+  int precision;   /* TABI_PREC_* */
+  int flags;       /* reserved, 0 */
+} tabi_params;
+
+/* Fills p with the reference defaults: order 3, maxparnode 500, theta 0.8,
+ * eps 1/80, 0.15 M (kappa from tabi_kappa), iprcd 1, tol 1e-4, maxl 10,
+ * nrmax 10, FP64. */
+void tabi_default_params(tabi_params* p);
+
+/* main.f90:62-63: kappa = sqrt(8.430325455 * I / eps1) with the literal
+ * rounded to REAL*4 as the Fortran does. */
+double tabi_kappa(double bulk_strength, double eps1);
+
+int tabi_create(tabi_h* h, const tabi_params* p);
+int tabi_destroy(tabi_h h);
+const char* tabi_last_error(tabi_h h);
+
+/* main.f90:546-610 form_matrix.  sptpos/sptnrm: 3 x nspt vertices and
+ * vertex normals (MSMS .vert), nvert: 3 x nface 1-based (MSMS .face, already
+ * filtered by readin.f90:264-333 surface_area), chrpos: 3 x nchr, atmchr:
+ * nchr.  Outputs (original face order): tr_xyz, tr_q (3 x nface centroids and
+ * unit normals), tr_area (nface), bvct (2 nface).  Any output may be NULL.
+ * Also loads the surface into the handle (replaces tabi_set_surface). */
+int tabi_form_matrix(tabi_h h, int nspt, const double* sptpos,
+                     const double* sptnrm, int nface, const int* nvert,
+                     int nchr, const double* chrpos, const double* atmchr,
+                     double* tr_xyz, double* tr_q, double* tr_area,
+                     double* bvct);
+
+/* Loads centroids, unit normals and areas (original order) when the caller
+ * already has them (the state form_matrix leaves in module treecode). */
+int tabi_set_surface(tabi_h h, int nface, const double* tr_xyz,
+                     const double* tr_q, const double* tr_area);
+
+/* main.f90:597-607: the RHS of form_matrix alone, for the loaded surface,
+ * in the CURRENT order of the handle (original order before
+ * tabi_build_tree, tree order after). */
+int tabi_rhs(tabi_h h, int nchr, const double* chrpos, const double* atmchr,
+             double* bvct);
+
+/* main.f90:400-441 SETUP + CREATE_TREE (treecode3d_pb.f:54-356): builds the
+ * tree on the device (same node sets, boxes and children order as the
+ * reference), the interaction lists and the preconditioner factors.
+ * orderarr (may be NULL) receives, per tree slot, the 1-based original face
+ * index; the caller then permutes its arrays as main.f90:447-453 does.  The
+ * order of faces inside a leaf may differ from the reference's (its
+ * PARTITION is not stable); node sets are identical. */
+int tabi_build_tree(tabi_h h, int* orderarr, int* nleaf);
+
+/* main.f90:467-488 MATVECmain -> TREE_COMPP_PB (treecode3d_pb.f:1130-1189):
+ * y = A x with A the treecode BIE operator; an x with sum|x| < 1e-10 gives
+ * y = x as in the reference.  n2 = 2 nface. */
+int tabi_matvec(tabi_h h, int n2, const double* x, double* y);
+int tabi_matvec_dev(tabi_h h, int n2, const double* x_dev, double* y_dev,
+                    void* stream);
+
+/* main.f90:511-529 MSOLVEdric -> LEAFMATVECpara (treecode3d_pb.f:1393-1542)
+ * when iprcd == 1, else main.f90:532-542 MSOLVEprec.  The leaf blocks are
+ * factored once in tabi_build_tree (the reference re-factors the same blocks
+ * on every call; the factors are identical). */
+int tabi_msolve(tabi_h h, int n2, const double* r, double* z);
+int tabi_msolve_dev(tabi_h h, int n2, const double* r_dev, double* z_dev,
+                    void* stream);
+
+/* main.f90:92-139 + dgmres_dep.f DGMRES (ITOL = 2, JPRE = -1, JSCAL = 0,
+ * KMP = MAXL): x holds x0 on entry (the reference uses 0).  iter, err, ierr
+ * as DGMRES returns them (ierr 0 converged, 1 iteration limit, 2 stagnation,
+ * -1/-2 as in dgmres_dep.f:840-851).  err_hist (may be NULL, capacity
+ * (nrmax+1)*maxl) receives the per-iteration error estimates the reference
+ * prints at dgmres_dep.f:1796; *n_hist their count. */
+int tabi_solve(tabi_h h, int n2, const double* b, double* x, int* iter,
+               double* err, int* ierr, double* err_hist, int* n_hist);
+int tabi_solve_dev(tabi_h h, int n2, const double* b_dev, double* x_dev,
+                   int* iter, double* err, int* ierr, double* err_hist,
+                   int* n_hist, void* stream);
+
+/* main.f90:144-157 + potential_molecule (main.f90:614-657): solvation energy
+ * soleng and Coulomb energy couleng (kcal/mol) for the solution x (tree
+ * order, as tabi_solve returns it). */
+int tabi_energy(tabi_h h, int nchr, const double* chrpos,
+                const double* atmchr, const double* x, double* soleng,
+                double* couleng);
+int tabi_energy_dev(tabi_h h, int nchr, const double* chrpos_dev,
+                    const double* atmchr_dev, const double* x_dev,
+                    double* soleng, double* couleng, void* stream);
+
+/* Whole path on device-resident inputs (form_matrix, tree, preconditioner,
+ * GMRES, energy) -- one call per molecule.  Inputs as tabi_form_matrix but
+ * device pointers; x_dev (2 nface, tree order on return) may be NULL.
+ * stats (may be NULL) receives: [0] iter, [1] err, [2] ierr, [3] soleng,
+ * [4] couleng, [5] near pairs per matvec, [6] far interactions per matvec,
+ * [7] nleaf. */
+int tabi_run_dev(tabi_h h, int nspt, const double* sptpos_dev,
+                 const double* sptnrm_dev, int nface, const int* nvert_dev,
+                 int nchr, const double* chrpos_dev, const double* atmchr_dev,
+                 double* x_dev, double* stats, void* stream);
+
+/* Interaction counts of the current tree (per matvec): near-field pairs and
+ * far-field (target, cluster) evaluations; as the reference's traversal
+ * would perform them. */
+int tabi_counts(tabi_h h, int64_t* near_pairs, int64_t* far_interactions);
+
+/* Node table of the current tree in depth-first (reference creation) order:
+ * ibeg (1-based), numpar, level, num_children, and geo = x_mid, y_mid,
+ * z_mid, radius per node.  Pass NULL arrays to get *nnodes only. */
+int tabi_tree_nodes(tabi_h h, int* nnodes, int* ibeg, int* numpar,
+                    int* level, int* nchild, double* geo);
+
+/* Instrumentation (no counterpart in the reference, which only prints
+ * cpu_time totals): every kernel launch of the library is counted per kernel
+ * class; while profiling is enabled each launch is also timed with CUDA
+ * events recorded on the stream it is launched on.  tabi_profile_enable
+ * resets the counters.  kclass -1 reads the sum over all classes. */
+int tabi_profile_enable(tabi_h h, int enable);
+int tabi_profile_read(tabi_h h, int kclass, double* ms, int64_t* launches);
+int tabi_profile_nclasses(void);
+const char* tabi_profile_class_name(int kclass);
+
+/* FP64 pipe peak probe: runs a DFMA loop for about `ms` milliseconds and
+ * returns the achieved FP64 FLOP/s (2 per FMA). */
+int tabi_probe_fp64_peak(double ms, double* flops);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TABI_GPU_H */

@@ -1,0 +1,303 @@
+// gmres.cu -- restarted, left-preconditioned GMRES with the semantics of the
+// reference's vendored SLATEC DGMRES (dgmres_dep.f) as main.f90:92-137 calls
+// it: ITOL = 2 (stop when |M^-1 (b - A x)| / |M^-1 b| <= tol), JPRE = -1,
+// JSCAL = 0, KMP = MAXL (full modified Gram-Schmidt), restarts from the
+// recurrence residual.  The small Hessenberg / Givens work (DHEQR, DHELS) runs
+// on the host exactly as SLATEC does it; every length-2N vector operation
+// runs on the device:
+//   DORTH (dgmres_dep.f:1376-1415)  dot -> device slot, axpy reading that slot,
+//                                    so one host round trip per iteration,
+//   DRLCAL (:1948-1979)             the residual recurrence collapsed into one
+//                                    linear combination of the Krylov vectors,
+//                                    fused with its norm (ISDGMR :2532-2650),
+//   DPIGMR final update (:1836-1848) one linear combination.
+#include <cmath>
+#include <vector>
+
+#include "reduce.cuh"
+#include "tabi_impl.cuh"
+
+namespace tabi {
+
+double reduce_dev(Handle& H, int op, const double* a, const double* b, int n, cudaStream_t s);
+
+namespace {
+
+struct Coefs {
+  double c[64];
+};
+
+__global__ void __launch_bounds__(kRedThreads) lincomb_kernel(const double* __restrict__ V,
+                                                              int64_t ld, int n, int nv,
+                                                              Coefs cf, double* __restrict__ out,
+                                                              double* __restrict__ part) {
+  double acc = 0.0;
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    double v = 0.0;
+    for (int j = 0; j < nv; ++j) v = fma(cf.c[j], V[(int64_t)j * ld + i], v);
+    out[i] = v;
+    acc = fma(v, v, acc);
+  }
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  __shared__ double s[kRedThreads / 32];
+  if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0 && part) {
+    double t = 0.0;
+    for (int k = 0; k < kRedThreads / 32; ++k) t += s[k];
+    part[blockIdx.x] = t;
+  }
+}
+
+// y += sign * (*coef) * x
+__global__ void axpy_dcoef_kernel(int n, const double* __restrict__ coef, double sign,
+                                  const double* __restrict__ x, double* __restrict__ y) {
+  double a = sign * (*coef);
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = fma(a, x[i], y[i]);
+}
+__global__ void axpy_kernel(int n, double a, const double* __restrict__ x,
+                            double* __restrict__ y) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    y[i] = fma(a, x[i], y[i]);
+}
+__global__ void scal_kernel(int n, double a, double* __restrict__ x) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    x[i] = a * x[i];
+}
+__global__ void sub_kernel(int n, const double* __restrict__ b, double* __restrict__ r) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
+    r[i] = b[i] - r[i];
+}
+
+constexpr int kVecBlocks = 592;
+
+void givens(double t1, double t2, double& c, double& s) {
+  if (t2 == 0.0) {
+    c = 1.0;
+    s = 0.0;
+  } else if (std::fabs(t2) >= std::fabs(t1)) {
+    double t = t1 / t2;
+    s = -1.0 / std::sqrt(1.0 + t * t);
+    c = -s * t;
+  } else {
+    double t = t2 / t1;
+    c = 1.0 / std::sqrt(1.0 + t * t);
+    s = -c * t;
+  }
+}
+
+}  // namespace
+
+void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err_out,
+               int* ierr_out, double* hist, int* nhist, cudaStream_t s) {
+  const int n = 2 * H.n;
+  int maxl = H.prm.maxl;
+  if (maxl == 0) maxl = 10;
+  if (maxl > n) maxl = n;
+  TABI_REQUIRE(maxl <= 60, TABI_ERR_ARG, "maxl must be <= 60");
+  const int kmp = maxl;
+  int nrmax = H.prm.nrmax;
+  if (nrmax == 0) nrmax = 10;
+  if (nrmax == -1) nrmax = 0;
+  double tol = H.prm.tol;
+  if (tol == 0.0) tol = 500 * 1e-20;
+  const int maxlp1 = maxl + 1, ldh = maxlp1;
+  H.d_v.alloc((size_t)n * maxlp1);
+  H.d_wk.alloc(n);
+  H.d_dl.alloc(n);
+  H.d_gz.alloc(n);
+  H.d_r.alloc(n);
+  H.d_coef.alloc(4 * (size_t)maxlp1 + kRedBlocks + 8);
+  H.d_red.alloc(kRedBlocks + 8);
+  double* V = H.d_v.p;
+  double* wk = H.d_wk.p;
+  double* dl = H.d_dl.p;
+  double* z = H.d_gz.p;
+  double* r = H.d_r.p;
+  double* d_h = H.d_coef.p;                       // HES column slots
+  double* d_part = H.d_coef.p + 4 * maxlp1;       // partial sums
+  std::vector<double> hes((size_t)maxlp1 * maxl), q(2 * maxl), r0ls(maxlp1 + 1);
+  auto HES = [&](int i, int j) -> double& { return hes[(size_t)(j - 1) * ldh + (i - 1)]; };
+  auto Vc = [&](int j) { return V + (size_t)(j - 1) * n; };
+  const int vb = kVecBlocks, vt = 256;
+  auto lincomb_norm = [&](int nv, const Coefs& cf, double* out, bool want_norm) -> double {
+    int nb = std::min(kRedBlocks, ceil_div(n, kRedThreads));
+    { TABI_K(K_VEC, s); lincomb_kernel<<<nb, kRedThreads, 0, s>>>(V, n, n, nv, cf, out, want_norm ? d_part : nullptr); }
+    if (!want_norm) return 0.0;
+    { TABI_K(K_VEC, s); reduce_final_kernel<<<1, 256, 0, s>>>(d_part, nb, d_part + kRedBlocks); }
+    TABI_CUDA(cudaMemcpyAsync(H.h_pinned, d_part + kRedBlocks, sizeof(double),
+                              cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+    return std::sqrt(H.h_pinned[0]);
+  };
+
+  int iter = 0, ierr = 0, nh = 0;
+  double err = 0.0;
+  int nrsts = 0;
+  // DGMRES :754-781: BNRM = |M^-1 b|, r = b - A x
+  msolve_dev(H, b, r, s);
+  double bnrm = nrm2_dev(H, r, n, s);
+  matvec_dev(H, x, r, s, true);
+  { TABI_K(K_VEC, s); sub_kernel<<<vb, vt, 0, s>>>(n, b, r); }
+  for (;;) {
+    if (nrsts > nrmax) {
+      ierr = 1;
+      break;
+    }
+    if (nrsts > 0) TABI_CUDA(cudaMemcpyAsync(r, dl, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    // ---- DPIGMR
+    int iflag = 0, lgmr = 0;
+    double snormw = 0.0, prod = 1.0, rho = 0.0;
+    if (nrsts == 0) {
+      TABI_CUDA(cudaMemcpyAsync(wk, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+      msolve_dev(H, wk, r, s);
+    }
+    TABI_CUDA(cudaMemcpyAsync(Vc(1), r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
+    double r0nrm = nrm2_dev(H, Vc(1), n, s);
+    err = r0nrm / bnrm;  // ISDGMR with LGMR = 0
+    bool zero_z = true;
+    if (!(err <= tol)) {
+      { TABI_K(K_VEC, s); scal_kernel<<<vb, vt, 0, s>>>(n, 1.0 / r0nrm, Vc(1)); }
+      std::fill(hes.begin(), hes.end(), 0.0);
+      prod = 1.0;
+      bool go200 = false, go120 = false;
+      for (int ll = 1; ll <= maxl; ++ll) {
+        lgmr = ll;
+        double* vn = Vc(ll + 1);
+        matvec_dev(H, Vc(ll), wk, s, false);  // |V(:,ll)| = 1: never the zero shortcut
+        msolve_dev(H, wk, vn, s);
+        // ---- DORTH
+        { TABI_K(K_VEC, s); reduce_partial_kernel<2><<<kRedBlocks, kRedThreads, 0, s>>>(vn, nullptr, n, d_part); }
+        { TABI_K(K_VEC, s); reduce_final_kernel<<<1, 256, 0, s>>>(d_part, kRedBlocks, d_h + maxlp1); }  // vnrm^2
+        int i0 = std::max(1, ll - kmp + 1);
+        for (int i = i0; i <= ll; ++i) {
+          { TABI_K(K_VEC, s); reduce_partial_kernel<1><<<kRedBlocks, kRedThreads, 0, s>>>(Vc(i), vn, n, d_part); }
+          { TABI_K(K_VEC, s); reduce_final_kernel<<<1, 256, 0, s>>>(d_part, kRedBlocks, d_h + (i - 1)); }
+          { TABI_K(K_VEC, s); axpy_dcoef_kernel<<<vb, vt, 0, s>>>(n, d_h + (i - 1), -1.0, Vc(i), vn); }
+        }
+        { TABI_K(K_VEC, s); reduce_partial_kernel<2><<<kRedBlocks, kRedThreads, 0, s>>>(vn, nullptr, n, d_part); }
+        { TABI_K(K_VEC, s); reduce_final_kernel<<<1, 256, 0, s>>>(d_part, kRedBlocks, d_h + maxlp1 + 1); }
+        TABI_CUDA(cudaMemcpyAsync(H.h_pinned, d_h, sizeof(double) * (maxlp1 + 2),
+                                  cudaMemcpyDeviceToHost, s));
+        TABI_CUDA(cudaStreamSynchronize(s));
+        for (int i = i0; i <= ll; ++i) HES(i, ll) = H.h_pinned[i - 1];
+        double vnrm = std::sqrt(H.h_pinned[maxlp1]);
+        snormw = std::sqrt(H.h_pinned[maxlp1 + 1]);
+        if (!(vnrm + 0.001 * snormw != vnrm)) {
+          // conditional re-orthogonalisation (dgmres_dep.f:1397-1414)
+          double sumdsq = 0.0;
+          for (int i = i0; i <= ll; ++i) {
+            double tem = -dot_dev(H, Vc(i), vn, n, s);
+            if (HES(i, ll) + 0.001 * tem == HES(i, ll)) continue;
+            HES(i, ll) = HES(i, ll) - tem;
+            { TABI_K(K_VEC, s); axpy_kernel<<<vb, vt, 0, s>>>(n, tem, Vc(i), vn); }
+            sumdsq += tem * tem;
+          }
+          if (sumdsq != 0.0) snormw = std::sqrt(std::max(0.0, snormw * snormw - sumdsq));
+        }
+        HES(ll + 1, ll) = snormw;
+        // ---- DHEQR (IJOB = 1 for ll = 1, else 2)
+        int info = 0;
+        for (int k = 1; k <= ll - 1; ++k) {
+          double t1 = HES(k, ll), t2 = HES(k + 1, ll);
+          double c = q[2 * (k - 1)], sn = q[2 * (k - 1) + 1];
+          HES(k, ll) = c * t1 - sn * t2;
+          HES(k + 1, ll) = sn * t1 + c * t2;
+        }
+        {
+          double c, sn, t1 = HES(ll, ll), t2 = HES(ll + 1, ll);
+          givens(t1, t2, c, sn);
+          q[2 * ll - 2] = c;
+          q[2 * ll - 1] = sn;
+          HES(ll, ll) = c * t1 - sn * t2;
+          if (HES(ll, ll) == 0.0) info = ll;
+        }
+        if (info == ll) {
+          go120 = true;
+          break;
+        }
+        prod = prod * q[2 * ll - 1];
+        rho = std::fabs(prod * r0nrm);
+        // ---- ISDGMR with DRLCAL: dl = r0nrm*prod * (recurrence of V columns)
+        Coefs cf{};
+        cf.c[0] = 1.0;
+        for (int i = 1; i <= ll - 1; ++i) {
+          double sn = q[2 * i - 1], c = q[2 * i - 2];
+          for (int j = 0; j < i; ++j) cf.c[j] *= sn;
+          cf.c[i] += c;
+        }
+        {
+          double sn = q[2 * ll - 1], c = q[2 * ll - 2] / snormw;
+          for (int j = 0; j < ll; ++j) cf.c[j] *= sn;
+          cf.c[ll] += c;
+        }
+        for (int j = 0; j <= ll; ++j) cf.c[j] *= r0nrm * prod;
+        double rl = lincomb_norm(ll + 1, cf, dl, true);
+        err = rl / bnrm;
+        if (hist) hist[nh] = err;
+        nh++;
+        if (err <= tol) {
+          go200 = true;
+          break;
+        }
+        if (ll == maxl) break;
+        { TABI_K(K_VEC, s); scal_kernel<<<vb, vt, 0, s>>>(n, 1.0 / snormw, vn); }
+      }
+      if (!go200 && !go120) {
+        if (rho < r0nrm) {
+          iflag = 1;
+          // DRLCAL(MAXL) at label 150: already in dl from the last iteration
+          go200 = true;
+        } else {
+          go120 = true;
+        }
+      }
+      if (go120) {
+        iflag = 2;
+      } else {
+        // DHELS (dgmres_dep.f:925-950) and z = V(:,1:lgmr) * y
+        int l = lgmr;
+        std::fill(r0ls.begin(), r0ls.end(), 0.0);
+        r0ls[0] = r0nrm;
+        for (int k = 1; k <= l; ++k) {
+          double c = q[2 * (k - 1)], sn = q[2 * (k - 1) + 1];
+          double t1 = r0ls[k - 1], t2 = r0ls[k];
+          r0ls[k - 1] = c * t1 - sn * t2;
+          r0ls[k] = sn * t1 + c * t2;
+        }
+        for (int kb = 1; kb <= l; ++kb) {
+          int k = l + 1 - kb;
+          r0ls[k - 1] = r0ls[k - 1] / HES(k, k);
+          double t = -r0ls[k - 1];
+          for (int i = 1; i <= k - 1; ++i) r0ls[i - 1] += t * HES(i, k);
+        }
+        Coefs cf{};
+        for (int i = 0; i < l; ++i) cf.c[i] = r0ls[i];
+        lincomb_norm(l, cf, z, false);
+        zero_z = false;
+      }
+    }
+    // ---- DGMRES :796-814
+    iter += lgmr;
+    if (!zero_z) { TABI_K(K_VEC, s); axpy_kernel<<<vb, vt, 0, s>>>(n, 1.0, z, x); }
+    if (iflag == 0) {
+      ierr = 0;
+      break;
+    }
+    if (iflag == 1) {
+      nrsts++;
+      continue;
+    }
+    ierr = 2;
+    break;
+  }
+  TABI_CUDA(cudaStreamSynchronize(s));
+  TABI_CUDA(cudaGetLastError());
+  *iter_out = iter;
+  *err_out = err;
+  *ierr_out = ierr;
+  if (nhist) *nhist = nh;
+}
+
+}  // namespace tabi

@@ -1,0 +1,317 @@
+// matvec.cu -- the treecode operator y = A x (TREE_COMPP_PB,
+// treecode3d_pb.f:1130-1189) as four device steps:
+//
+//  1. moments   COMP_MS (treecode3d_pb.f:859-916) for every cluster some
+//               target accepts.  The 16 source charges of pb_kernel
+//               (main.f90:664-694) reduce to 4 distinct ones -- A*x2 and
+//               (n_d*A)*x1 -- so 4 raw moment sets are summed, then
+//               weighted by the integer part of der_cof (main.f90:380-399)
+//               into the 16 per-index sets the contraction reads.
+//  2. far       one thread per (target, accepted cluster): the generated
+//               COMP_TCOEFF + COMPP_TREE_PB evaluation (taylor_gen.cuh),
+//               cluster moments staged in shared memory.
+//  3. near      one thread per (target, near leaf): COMPP_DIRECT_PB
+//               (treecode3d_pb.f:919-1008) over the leaf's faces staged in
+//               shared memory; the target's own face is skipped, which is what
+//               the reference's shift-and-zero-area trick (:1169-1172) amounts
+//               to.
+//  4. reduce    per target, the interaction results summed in traversal order:
+//               y1 = pre1*x1 - peng1, y2 = pre2*x2 - peng2 (:1177-1178).
+// All results are written to per-(target, interaction) slots fixed by the
+// traversal, so the sums are deterministic.
+#include "bie_kernels.cuh"
+#include "reduce.cuh"
+#include "taylor_gen.cuh"
+#include "tabi_impl.cuh"
+
+namespace tabi {
+
+namespace {
+
+// ---- moments
+template <int P>
+__global__ void mom_partial_kernel(const int4* __restrict__ chunks,
+                                   const int* __restrict__ mslot_node,
+                                   const double* __restrict__ nd_mid,
+                                   const double* __restrict__ px, const double* __restrict__ py,
+                                   const double* __restrict__ pz, const double* __restrict__ nx,
+                                   const double* __restrict__ ny, const double* __restrict__ nz,
+                                   const double* __restrict__ area,
+                                   const double* __restrict__ x, int n,
+                                   double* __restrict__ mraw) {
+  constexpr int NT = tabi_nterms(P);
+  constexpr int TILE = 128;
+  constexpr int W = 3 * (P + 1) + 4;
+  __shared__ double st[TILE][W];
+  int4 ch = chunks[blockIdx.x];
+  int node = mslot_node[ch.x];
+  double mx = nd_mid[3 * node], my = nd_mid[3 * node + 1], mz = nd_mid[3 * node + 2];
+  int t = threadIdx.x;
+  int set = t / NT, term = t - set * NT;
+  bool own = t < 4 * NT;
+  int k1 = 0, k2 = 0, k3 = 0;
+  if (own) {
+    const signed char(*tt)[3] = tabi_terms<P>();
+    k1 = tt[term][0];
+    k2 = tt[term][1];
+    k3 = tt[term][2];
+  }
+  double acc = 0.0;
+  for (int base = 0; base < ch.z; base += TILE) {
+    int cnt = min(TILE, ch.z - base);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+      int i = ch.y + base + q;
+      // COMP_MS :876-889: dx = x - mid, powers by repeated multiplication
+      double dx = px[i] - mx, dy = py[i] - my, dz = pz[i] - mz;
+      double a = 1.0, b = 1.0, c = 1.0;
+#pragma unroll
+      for (int p = 0; p <= P; ++p) {
+        st[q][p] = a;
+        st[q][P + 1 + p] = b;
+        st[q][2 * (P + 1) + p] = c;
+        a *= dx;
+        b *= dy;
+        c *= dz;
+      }
+      double A = area[i], x1 = x[i], x2 = x[n + i];
+      // pb_kernel (main.f90:673-681): A*x2 and (n_d*A)*x1
+      st[q][3 * (P + 1) + 0] = A * x2;
+      st[q][3 * (P + 1) + 1] = (nx[i] * A) * x1;
+      st[q][3 * (P + 1) + 2] = (ny[i] * A) * x1;
+      st[q][3 * (P + 1) + 3] = (nz[i] * A) * x1;
+    }
+    __syncthreads();
+    if (own)
+      for (int q = 0; q < cnt; ++q) {
+        double txyz = st[q][k1] * st[q][P + 1 + k2] * st[q][2 * (P + 1) + k3];
+        acc = fma(st[q][3 * (P + 1) + set], txyz, acc);
+      }
+  }
+  if (own) mraw[((size_t)ch.w * 4 + set) * NT + term] = acc;
+}
+
+template <int P>
+__global__ void mom_final_kernel(const int2* __restrict__ mslot_chunks,
+                                 const double* __restrict__ mraw, double* __restrict__ mw) {
+  constexpr int NT = tabi_nterms(P);
+  int slot = blockIdx.x;
+  int2 cr = mslot_chunks[slot];
+  const signed char(*tt)[3] = tabi_terms<P>();
+  // kk (main.f90:358-376) and the source set / sign of each of the 16 indices
+  const int kk[16][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 0}, {0, 1, 0},
+                         {0, 0, 1}, {2, 0, 0}, {1, 1, 0}, {1, 0, 1}, {1, 1, 0}, {0, 2, 0},
+                         {0, 1, 1}, {1, 0, 1}, {0, 1, 1}, {0, 0, 2}};
+  for (int q = threadIdx.x; q < 16 * NT; q += blockDim.x) {
+    int idx = q / NT, term = q - idx * NT;
+    int set = (idx == 0) ? 0 : (idx <= 3) ? idx : (idx <= 6) ? 0 : 1 + (idx - 7) / 3;
+    double sgn = (idx >= 7) ? -1.0 : 1.0;
+    double raw = 0.0;
+    for (int c = 0; c < cr.y; ++c) raw += mraw[((size_t)(cr.x + c) * 4 + set) * NT + term];
+    int kv[3] = {tt[term][0], tt[term][1], tt[term][2]};
+    double w = 1.0;
+    for (int m = 0; m < 3; ++m)
+      for (int j = 1; j <= kk[idx][m]; ++j) w *= (double)(kv[m] + j);
+    mw[(size_t)slot * 16 * NT + q] = sgn * w * raw;
+  }
+}
+
+// ---- far field
+template <int P>
+__global__ void __launch_bounds__(64) far_kernel(const WorkItem* __restrict__ work,
+                                                 const int2* __restrict__ ent,
+                                                 const double* __restrict__ mw,
+                                                 const double* __restrict__ nd_mid,
+                                                 const double* __restrict__ px,
+                                                 const double* __restrict__ py,
+                                                 const double* __restrict__ pz,
+                                                 const double* __restrict__ nx,
+                                                 const double* __restrict__ ny,
+                                                 const double* __restrict__ nz, double kappa,
+                                                 double eps, double2* __restrict__ res) {
+  constexpr int NT = tabi_nterms(P);
+  __shared__ double smw[16 * NT];
+  WorkItem wi = work[blockIdx.x];
+  const double* src = mw + (size_t)wi.mslot * 16 * NT;
+  for (int q = threadIdx.x; q < 16 * NT; q += blockDim.x) smw[q] = src[q];
+  __syncthreads();
+  if ((int)threadIdx.x >= wi.count) return;
+  int2 e = ent[wi.start + threadIdx.x];
+  int t = e.x;
+  // COMP_TCOEFF :707-709: dx = target - mid
+  double dx = px[t] - nd_mid[3 * wi.node];
+  double dy = py[t] - nd_mid[3 * wi.node + 1];
+  double dz = pz[t] - nd_mid[3 * wi.node + 2];
+  double o1, o2;
+  far_eval<P, double>(dx, dy, dz, kappa, smw, nx[t], ny[t], nz[t], eps, 1.0 / eps, o1, o2);
+  res[e.y] = make_double2(o1 * kOneOver4Pi, o2 * kOneOver4Pi);
+}
+
+// ---- near field
+constexpr int kNearThreads = 128;
+constexpr int kNearTile = 256;
+
+__global__ void __launch_bounds__(kNearThreads) near_kernel(
+    const WorkItem* __restrict__ work, const int2* __restrict__ ent,
+    const int* __restrict__ nd_ibeg, const int* __restrict__ nd_num,
+    const double* __restrict__ px, const double* __restrict__ py,
+    const double* __restrict__ pz, const double* __restrict__ nx,
+    const double* __restrict__ ny, const double* __restrict__ nz,
+    const double* __restrict__ area, const double* __restrict__ x, int n, double kappa,
+    double eps, double2* __restrict__ res) {
+  __shared__ double s_x[kNearTile], s_y[kNearTile], s_z[kNearTile];
+  __shared__ double s_nx[kNearTile], s_ny[kNearTile], s_nz[kNearTile];
+  __shared__ double s_w1[kNearTile], s_w2[kNearTile];
+  WorkItem wi = work[blockIdx.x];
+  int ib = nd_ibeg[wi.node], nsrc = nd_num[wi.node];
+  bool own = (int)threadIdx.x < wi.count;
+  int t = 0, slot = 0;
+  double tx = 0, ty = 0, tz = 0, vx = 0, vy = 0, vz = 0;
+  if (own) {
+    int2 e = ent[wi.start + threadIdx.x];
+    t = e.x;
+    slot = e.y;
+    tx = px[t];
+    ty = py[t];
+    tz = pz[t];
+    vx = nx[t];
+    vy = ny[t];
+    vz = nz[t];
+  }
+  const double inv_eps = 1.0 / eps;
+  double p1 = 0.0, p2 = 0.0;
+  for (int b0 = 0; b0 < nsrc; b0 += kNearTile) {
+    int cnt = min(kNearTile, nsrc - b0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+      int j = ib + b0 + q;
+      s_x[q] = px[j];
+      s_y[q] = py[j];
+      s_z[q] = pz[j];
+      s_nx[q] = nx[j];
+      s_ny[q] = ny[j];
+      s_nz[q] = nz[j];
+      double A = area[j];
+      s_w1[q] = A * x[j];
+      s_w2[q] = A * x[n + j];
+    }
+    __syncthreads();
+    if (own) {
+      int self = t - (ib + b0);
+#pragma unroll 2
+      for (int q = 0; q < cnt; ++q) {
+        bool skip = (q == self);
+        double dx = s_x[q] - tx, dy = s_y[q] - ty, dz = s_z[q] - tz;
+        if (skip) dx = 1.0;  // keeps the skipped pair finite
+        double K1, K2, K3, K4;
+        bie4<double>(dx, dy, dz, vx, vy, vz, s_nx[q], s_ny[q], s_nz[q], kappa, eps, inv_eps, K1,
+                     K2, K3, K4);
+        double w1 = skip ? 0.0 : s_w1[q], w2 = skip ? 0.0 : s_w2[q];
+        p1 = fma(K1, w1, fma(K2, w2, p1));
+        p2 = fma(K3, w1, fma(K4, w2, p2));
+      }
+    }
+  }
+  if (own) res[slot] = make_double2(p1, p2);
+}
+
+__global__ void reduce_kernel(const int64_t* __restrict__ slot_off,
+                              const double2* __restrict__ res, const double* __restrict__ x,
+                              int n, double pre1, double pre2, double* __restrict__ y) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n) return;
+  double s1 = 0.0, s2 = 0.0;
+  for (int64_t k = slot_off[t]; k < slot_off[t + 1]; ++k) {
+    double2 r = res[k];
+    s1 += r.x;
+    s2 += r.y;
+  }
+  y[t] = pre1 * x[t] - s1;
+  y[n + t] = pre2 * x[n + t] - s2;
+}
+
+template <int P>
+void launch_order(Handle& H, const double* x, double* y, cudaStream_t s) {
+  Tree& T = H.tree;
+  const int n = H.n;
+  constexpr int NT = tabi_nterms(P);
+  if (T.nmslot > 0) {
+    int nch = 0;
+    for (int k = 0; k < T.nmslot; ++k) nch += T.mslot_nchunk[k];
+    int threads = ((4 * NT + 31) / 32) * 32;
+    { TABI_K(K_MOMENTS, s); mom_partial_kernel<P><<<nch, threads, 0, s>>>(T.d_mchunks.p, T.d_mslot_node.p, T.d_mid.p,
+                                                  H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p,
+                                                  H.d_ny.p, H.d_nz.p, H.d_area.p, x, n,
+                                                  H.d_mraw.p); }
+    { TABI_K(K_MOMENTS, s); mom_final_kernel<P><<<T.nmslot, 256, 0, s>>>(T.d_mslot_chunks.p, H.d_mraw.p, H.d_mw.p); }
+  }
+  if (!T.far_work.empty())
+    { TABI_K(K_FAR, s); far_kernel<P><<<(int)T.far_work.size(), 64, 0, s>>>(
+        T.d_far_work.p, T.d_far_ent.p, H.d_mw.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p,
+        H.d_nx.p, H.d_ny.p, H.d_nz.p, H.prm.kappa, H.prm.eps1 / H.prm.eps0, H.d_res.p); }
+}
+
+}  // namespace
+
+double reduce_dev(Handle& H, int op, const double* a, const double* b, int n, cudaStream_t s) {
+  H.d_red.alloc(kRedBlocks + 8);
+  int nb = std::min(kRedBlocks, ceil_div(n, kRedThreads));
+  if (nb < 1) nb = 1;
+  if (op == 0)
+    { TABI_K(K_VEC, s); reduce_partial_kernel<0><<<nb, kRedThreads, 0, s>>>(a, b, n, H.d_red.p); }
+  else if (op == 1)
+    { TABI_K(K_VEC, s); reduce_partial_kernel<1><<<nb, kRedThreads, 0, s>>>(a, b, n, H.d_red.p); }
+  else
+    { TABI_K(K_VEC, s); reduce_partial_kernel<2><<<nb, kRedThreads, 0, s>>>(a, b, n, H.d_red.p); }
+  { TABI_K(K_VEC, s); reduce_final_kernel<<<1, 256, 0, s>>>(H.d_red.p, nb, H.d_red.p + kRedBlocks); }
+  TABI_CUDA(cudaMemcpyAsync(H.h_pinned, H.d_red.p + kRedBlocks, sizeof(double),
+                            cudaMemcpyDeviceToHost, s));
+  TABI_CUDA(cudaStreamSynchronize(s));
+  return H.h_pinned[0];
+}
+
+double asum_dev(Handle& H, const double* x, int n, cudaStream_t s) {
+  return reduce_dev(H, 0, x, nullptr, n, s);
+}
+double dot_dev(Handle& H, const double* a, const double* b, int n, cudaStream_t s) {
+  return reduce_dev(H, 1, a, b, n, s);
+}
+double nrm2_dev(Handle& H, const double* a, int n, cudaStream_t s) {
+  return sqrt(reduce_dev(H, 2, a, nullptr, n, s));
+}
+
+void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool check_zero) {
+  const int n = H.n;
+  if (check_zero) {
+    // MATVECmain (main.f90:478-479): sum|x| < 1e-10 gives y = x
+    double a = asum_dev(H, x, 2 * n, s);
+    if (a < 1e-10) {
+      if (y != x)
+        TABI_CUDA(cudaMemcpyAsync(y, x, sizeof(double) * 2 * n, cudaMemcpyDeviceToDevice, s));
+      return;
+    }
+  }
+  Tree& T = H.tree;
+  switch (H.prm.order) {
+    case 1: launch_order<1>(H, x, y, s); break;
+    case 2: launch_order<2>(H, x, y, s); break;
+    case 3: launch_order<3>(H, x, y, s); break;
+    case 4: launch_order<4>(H, x, y, s); break;
+    case 5: launch_order<5>(H, x, y, s); break;
+    case 6: launch_order<6>(H, x, y, s); break;
+    case 7: launch_order<7>(H, x, y, s); break;
+    case 8: launch_order<8>(H, x, y, s); break;
+    default: throw Error(TABI_ERR_ARG, "order must be 1..8");
+  }
+  if (!T.near_work.empty())
+    { TABI_K(K_NEAR, s); near_kernel<<<(int)T.near_work.size(), kNearThreads, 0, s>>>(
+        T.d_near_work.p, T.d_near_ent.p, T.d_ibeg.p, T.d_num.p, H.d_x.p, H.d_y.p, H.d_z.p,
+        H.d_nx.p, H.d_ny.p, H.d_nz.p, H.d_area.p, x, n, H.prm.kappa,
+        H.prm.eps1 / H.prm.eps0, H.d_res.p); }
+  double eps = H.prm.eps1 / H.prm.eps0;
+  { TABI_K(K_REDUCE, s); reduce_kernel<<<ceil_div(n, 256), 256, 0, s>>>(T.d_slot_off.p, H.d_res.p, x, n,
+                                                 0.5 * (1.0 + eps), 0.5 * (1.0 + 1.0 / eps), y); }
+  TABI_CUDA(cudaGetLastError());
+}
+
+}  // namespace tabi

@@ -1,0 +1,602 @@
+// tabi_api.cu -- the C ABI (include/tabi_gpu.h): argument checks, host <-> device
+// staging, and the order of the steps main.f90 performs.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "tabi_impl.cuh"
+
+namespace tabi {
+void pack_atoms_dev(Handle& H, int nchr, const double* chrpos_dev, const double* atmchr_dev,
+                    cudaStream_t s);
+}
+
+using namespace tabi;
+
+struct tabi_handle_s {
+  Handle H;
+};
+
+namespace {
+
+thread_local std::string g_err;
+
+template <typename F>
+int guarded(tabi_h h, F&& f) {
+  try {
+    f();
+    if (h) h->H.err.clear();
+    return TABI_OK;
+  } catch (const Error& e) {
+    if (h) h->H.err = e.what();
+    g_err = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (h) h->H.err = "host allocation failed";
+    return TABI_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    if (h) h->H.err = e.what();
+    return TABI_ERR_CUDA;
+  }
+}
+
+cudaStream_t pick(Handle& H, void* stream) {
+  return stream ? (cudaStream_t)stream : H.stream;
+}
+
+void set_device(Handle& H) { TABI_CUDA(cudaSetDevice(H.device)); }
+
+void alloc_surface(Handle& H, int n) {
+  H.n = n;
+  H.d_x.alloc(n);
+  H.d_y.alloc(n);
+  H.d_z.alloc(n);
+  H.d_nx.alloc(n);
+  H.d_ny.alloc(n);
+  H.d_nz.alloc(n);
+  H.d_area.alloc(n);
+  H.has_surface = H.has_tree = H.has_precond = false;
+}
+
+__global__ void soa_from_aos_kernel(const double* xyz, const double* q, const double* area, int n,
+                                    double* x, double* y, double* z, double* nx, double* ny,
+                                    double* nz, double* a) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  x[i] = xyz[3 * (size_t)i];
+  y[i] = xyz[3 * (size_t)i + 1];
+  z[i] = xyz[3 * (size_t)i + 2];
+  nx[i] = q[3 * (size_t)i];
+  ny[i] = q[3 * (size_t)i + 1];
+  nz[i] = q[3 * (size_t)i + 2];
+  a[i] = area[i];
+}
+
+__global__ void aos_from_soa_kernel(const double* x, const double* y, const double* z,
+                                    const double* nx, const double* ny, const double* nz, int n,
+                                    double* xyz, double* q) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  xyz[3 * (size_t)i] = x[i];
+  xyz[3 * (size_t)i + 1] = y[i];
+  xyz[3 * (size_t)i + 2] = z[i];
+  q[3 * (size_t)i] = nx[i];
+  q[3 * (size_t)i + 1] = ny[i];
+  q[3 * (size_t)i + 2] = nz[i];
+}
+
+__global__ void permute_b_kernel(const int* perm, int n, const double* b, double* tb) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  int o = perm[i];
+  tb[i] = b[o];
+  tb[n + i] = b[n + o];
+}
+
+__global__ void fp64_peak_kernel(double* out, long iters) {
+  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
+  double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
+  const double m = 0.999999, c = 1e-7;
+  for (long i = 0; i < iters; ++i) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      a0 = fma(a0, m, c);
+      a1 = fma(a1, m, c);
+      a2 = fma(a2, m, c);
+      a3 = fma(a3, m, c);
+      a4 = fma(a4, m, c);
+      a5 = fma(a5, m, c);
+      a6 = fma(a6, m, c);
+      a7 = fma(a7, m, c);
+    }
+  }
+  double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == 123.456) out[0] = s;  // keeps the loop alive
+}
+
+void check_params(const tabi_params& p) {
+  TABI_REQUIRE(p.order >= 1 && p.order <= kMaxOrder, TABI_ERR_ARG, "order must be in 1..8");
+  TABI_REQUIRE(p.maxparnode >= 1, TABI_ERR_ARG, "maxparnode must be >= 1");
+  TABI_REQUIRE(p.theta > 0.0 && p.theta < 1.0, TABI_ERR_ARG,
+               "theta must be in (0, 1): the self-interaction removal of the reference needs "
+               "the MAC to fail on every cluster holding the target");
+  TABI_REQUIRE(p.kappa >= 0.0 && std::isfinite(p.kappa), TABI_ERR_ARG, "kappa must be >= 0");
+  TABI_REQUIRE(p.eps0 > 0.0 && p.eps1 > 0.0, TABI_ERR_ARG, "dielectrics must be > 0");
+  TABI_REQUIRE(p.maxl >= 0 && p.maxl <= 60, TABI_ERR_ARG, "maxl must be in 0..60");
+  TABI_REQUIRE(p.nrmax >= -1, TABI_ERR_ARG, "nrmax must be >= -1");
+  TABI_REQUIRE(p.tol >= 0.0, TABI_ERR_ARG, "tol must be >= 0");
+  TABI_REQUIRE(p.precision == TABI_PREC_FP64, TABI_ERR_ARG, "unsupported precision mode");
+  TABI_REQUIRE(p.maxparnode <= 12000, TABI_ERR_LIMIT, "maxparnode above 12000");
+}
+
+void require_tree(Handle& H, int n2) {
+  TABI_REQUIRE(H.has_tree, TABI_ERR_STATE, "tabi_build_tree has not been called");
+  TABI_REQUIRE(n2 == 2 * H.n, TABI_ERR_ARG, "vector length must be 2*nface");
+}
+
+void do_build(Handle& H, cudaStream_t s) {
+  build_tree(H, s);
+  build_lists(H, s);
+  H.has_tree = true;
+  build_precond(H, s);
+}
+
+template <typename T>
+void h2d(DBuf<T>& buf, const T* src, size_t n, cudaStream_t s) {
+  buf.alloc(std::max<size_t>(n, 1));
+  TABI_CUDA(cudaMemcpyAsync(buf.p, src, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+}
+
+}  // namespace
+
+extern "C" {
+
+void tabi_default_params(tabi_params* p) {
+  if (!p) return;
+  std::memset(p, 0, sizeof(*p));
+  p->order = 3;
+  p->maxparnode = 500;
+  p->theta = 0.8;
+  p->eps0 = 1.0;
+  p->eps1 = 80.0;
+  p->kappa = tabi_kappa(0.15, 80.0);
+  p->iprcd = 1;
+  p->tol = 1e-4;
+  p->maxl = 10;
+  p->nrmax = 10;
+  p->precision = TABI_PREC_FP64;
+}
+
+double tabi_kappa(double bulk_strength, double eps1) {
+  return std::sqrt((double)(float)8.430325455 * bulk_strength / eps1);
+}
+
+int tabi_create(tabi_h* h, const tabi_params* p) {
+  if (!h || !p) return TABI_ERR_ARG;
+  *h = nullptr;
+  tabi_h nh = nullptr;
+  int rc = guarded(nullptr, [&] {
+    check_params(*p);
+    int ndev = 0;
+    TABI_CUDA(cudaGetDeviceCount(&ndev));
+    TABI_REQUIRE(ndev > 0, TABI_ERR_CUDA, "no CUDA device");
+    nh = new tabi_handle_s();
+    nh->H.prm = *p;
+    TABI_CUDA(cudaGetDevice(&nh->H.device));
+    TABI_CUDA(cudaStreamCreateWithFlags(&nh->H.stream, cudaStreamNonBlocking));
+    TABI_CUDA(cudaMallocHost(&nh->H.h_pinned, sizeof(double) * 256));
+  });
+  if (rc != TABI_OK) {
+    if (nh) tabi_destroy(nh);
+    return rc;
+  }
+  *h = nh;
+  return TABI_OK;
+}
+
+int tabi_destroy(tabi_h h) {
+  if (!h) return TABI_OK;
+  cudaSetDevice(h->H.device);
+  if (h->H.stream) cudaStreamSynchronize(h->H.stream);
+  if (h->H.h_pinned) cudaFreeHost(h->H.h_pinned);
+  cudaStream_t s = h->H.stream;
+  delete h;
+  if (s) cudaStreamDestroy(s);
+  return TABI_OK;
+}
+
+const char* tabi_last_error(tabi_h h) { return h ? h->H.err.c_str() : g_err.c_str(); }
+
+int tabi_form_matrix(tabi_h h, int nspt, const double* sptpos, const double* sptnrm, int nface,
+                     const int* nvert, int nchr, const double* chrpos, const double* atmchr,
+                     double* tr_xyz, double* tr_q, double* tr_area, double* bvct) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(nspt > 0 && nface > 0 && nchr >= 0, TABI_ERR_ARG, "sizes must be positive");
+    TABI_REQUIRE(sptpos && sptnrm && nvert && (nchr == 0 || (chrpos && atmchr)), TABI_ERR_ARG,
+                 "null input array");
+    for (int k = 0; k < 3 * nface; ++k)
+      TABI_REQUIRE(nvert[k] >= 1 && nvert[k] <= nspt, TABI_ERR_ARG,
+                   "face vertex index out of range");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    alloc_surface(H, nface);
+    DBuf<double> dpos, dnrm, dcp, dq;
+    DBuf<int> dfv;
+    h2d(dpos, sptpos, 3 * (size_t)nspt, s);
+    h2d(dnrm, sptnrm, 3 * (size_t)nspt, s);
+    h2d(dfv, nvert, 3 * (size_t)nface, s);
+    if (nchr > 0) {
+      h2d(dcp, chrpos, 3 * (size_t)nchr, s);
+      h2d(dq, atmchr, (size_t)nchr, s);
+    }
+    pack_atoms_dev(H, nchr, dcp.p, dq.p, s);
+    DBuf<double> db;
+    db.alloc(2 * (size_t)nface);
+    launch_form_matrix(H, nspt, dpos.p, dnrm.p, nface, dfv.p, nchr, H.d_atoms.p, db.p, s);
+    if (tr_xyz || tr_q) {
+      DBuf<double> axyz, aq;
+      axyz.alloc(3 * (size_t)nface);
+      aq.alloc(3 * (size_t)nface);
+      { TABI_K(K_FORM, s); aos_from_soa_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(
+          H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p, H.d_ny.p, H.d_nz.p, nface, axyz.p, aq.p); }
+      if (tr_xyz)
+        TABI_CUDA(cudaMemcpyAsync(tr_xyz, axyz.p, sizeof(double) * 3 * nface,
+                                  cudaMemcpyDeviceToHost, s));
+      if (tr_q)
+        TABI_CUDA(cudaMemcpyAsync(tr_q, aq.p, sizeof(double) * 3 * nface,
+                                  cudaMemcpyDeviceToHost, s));
+      TABI_CUDA(cudaStreamSynchronize(s));
+    }
+    if (tr_area)
+      TABI_CUDA(cudaMemcpyAsync(tr_area, H.d_area.p, sizeof(double) * nface,
+                                cudaMemcpyDeviceToHost, s));
+    if (bvct)
+      TABI_CUDA(cudaMemcpyAsync(bvct, db.p, sizeof(double) * 2 * nface, cudaMemcpyDeviceToHost,
+                                s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+    H.has_surface = true;
+  });
+}
+
+int tabi_set_surface(tabi_h h, int nface, const double* tr_xyz, const double* tr_q,
+                     const double* tr_area) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(nface > 0 && tr_xyz && tr_q && tr_area, TABI_ERR_ARG, "bad surface arrays");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    alloc_surface(H, nface);
+    DBuf<double> a, b, c;
+    h2d(a, tr_xyz, 3 * (size_t)nface, s);
+    h2d(b, tr_q, 3 * (size_t)nface, s);
+    h2d(c, tr_area, (size_t)nface, s);
+    { TABI_K(K_FORM, s); soa_from_aos_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(a.p, b.p, c.p, nface, H.d_x.p,
+                                                             H.d_y.p, H.d_z.p, H.d_nx.p,
+                                                             H.d_ny.p, H.d_nz.p, H.d_area.p); }
+    TABI_CUDA(cudaStreamSynchronize(s));
+    H.has_surface = true;
+  });
+}
+
+int tabi_rhs(tabi_h h, int nchr, const double* chrpos, const double* atmchr, double* bvct) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(H.has_surface, TABI_ERR_STATE, "no surface loaded");
+    TABI_REQUIRE(nchr > 0 && chrpos && atmchr && bvct, TABI_ERR_ARG, "bad atom arrays");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    DBuf<double> dcp, dq, db;
+    h2d(dcp, chrpos, 3 * (size_t)nchr, s);
+    h2d(dq, atmchr, (size_t)nchr, s);
+    pack_atoms_dev(H, nchr, dcp.p, dq.p, s);
+    db.alloc(2 * (size_t)H.n);
+    launch_rhs(H, nchr, H.d_atoms.p, db.p, s);
+    TABI_CUDA(cudaMemcpyAsync(bvct, db.p, sizeof(double) * 2 * H.n, cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int tabi_build_tree(tabi_h h, int* orderarr, int* nleaf) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(H.has_surface, TABI_ERR_STATE, "no surface loaded");
+    TABI_REQUIRE(!H.has_tree, TABI_ERR_STATE, "tree already built for this surface");
+    set_device(H);
+    do_build(H, H.stream);
+    if (orderarr)
+      for (int i = 0; i < H.n; ++i) orderarr[i] = H.h_perm[i] + 1;
+    if (nleaf) *nleaf = H.tree.nleaf;
+  });
+}
+
+int tabi_matvec_dev(tabi_h h, int n2, const double* x_dev, double* y_dev, void* stream) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    require_tree(H, n2);
+    TABI_REQUIRE(x_dev && y_dev && x_dev != y_dev, TABI_ERR_ARG, "bad vectors");
+    set_device(H);
+    matvec_dev(H, x_dev, y_dev, pick(H, stream), true);
+  });
+}
+
+int tabi_matvec(tabi_h h, int n2, const double* x, double* y) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    require_tree(H, n2);
+    TABI_REQUIRE(x && y, TABI_ERR_ARG, "null vector");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    H.d_b.alloc(n2);
+    H.d_xio.alloc(n2);
+    TABI_CUDA(cudaMemcpyAsync(H.d_b.p, x, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+    matvec_dev(H, H.d_b.p, H.d_xio.p, s, true);
+    TABI_CUDA(cudaMemcpyAsync(y, H.d_xio.p, sizeof(double) * n2, cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int tabi_msolve_dev(tabi_h h, int n2, const double* r_dev, double* z_dev, void* stream) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    require_tree(H, n2);
+    TABI_REQUIRE(r_dev && z_dev, TABI_ERR_ARG, "bad vectors");
+    set_device(H);
+    msolve_dev(H, r_dev, z_dev, pick(H, stream));
+  });
+}
+
+int tabi_msolve(tabi_h h, int n2, const double* r, double* z) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    require_tree(H, n2);
+    TABI_REQUIRE(r && z, TABI_ERR_ARG, "null vector");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    H.d_b.alloc(n2);
+    H.d_xio.alloc(n2);
+    TABI_CUDA(cudaMemcpyAsync(H.d_b.p, r, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+    msolve_dev(H, H.d_b.p, H.d_xio.p, s);
+    TABI_CUDA(cudaMemcpyAsync(z, H.d_xio.p, sizeof(double) * n2, cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int tabi_solve_dev(tabi_h h, int n2, const double* b_dev, double* x_dev, int* iter, double* err,
+                   int* ierr, double* err_hist, int* n_hist, void* stream) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    require_tree(H, n2);
+    TABI_REQUIRE(b_dev && x_dev && iter && err && ierr, TABI_ERR_ARG, "null argument");
+    set_device(H);
+    gmres_dev(H, b_dev, x_dev, iter, err, ierr, err_hist, n_hist, pick(H, stream));
+  });
+}
+
+int tabi_solve(tabi_h h, int n2, const double* b, double* x, int* iter, double* err, int* ierr,
+               double* err_hist, int* n_hist) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    require_tree(H, n2);
+    TABI_REQUIRE(b && x && iter && err && ierr, TABI_ERR_ARG, "null argument");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    H.d_b.alloc(n2);
+    H.d_xio.alloc(n2);
+    TABI_CUDA(cudaMemcpyAsync(H.d_b.p, b, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+    TABI_CUDA(cudaMemcpyAsync(H.d_xio.p, x, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
+    gmres_dev(H, H.d_b.p, H.d_xio.p, iter, err, ierr, err_hist, n_hist, s);
+    TABI_CUDA(cudaMemcpyAsync(x, H.d_xio.p, sizeof(double) * n2, cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int tabi_energy_dev(tabi_h h, int nchr, const double* chrpos_dev, const double* atmchr_dev,
+                    const double* x_dev, double* soleng, double* couleng, void* stream) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(H.has_surface, TABI_ERR_STATE, "no surface loaded");
+    TABI_REQUIRE(nchr > 0 && chrpos_dev && atmchr_dev && x_dev && soleng && couleng,
+                 TABI_ERR_ARG, "bad energy arguments");
+    set_device(H);
+    cudaStream_t s = pick(H, stream);
+    pack_atoms_dev(H, nchr, chrpos_dev, atmchr_dev, s);
+    energy_dev(H, nchr, nullptr, nullptr, x_dev, soleng, couleng, s);
+  });
+}
+
+int tabi_energy(tabi_h h, int nchr, const double* chrpos, const double* atmchr, const double* x,
+                double* soleng, double* couleng) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(H.has_surface, TABI_ERR_STATE, "no surface loaded");
+    TABI_REQUIRE(nchr > 0 && chrpos && atmchr && x && soleng && couleng, TABI_ERR_ARG,
+                 "bad energy arguments");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    DBuf<double> dcp, dq, dx;
+    h2d(dcp, chrpos, 3 * (size_t)nchr, s);
+    h2d(dq, atmchr, (size_t)nchr, s);
+    h2d(dx, x, 2 * (size_t)H.n, s);
+    pack_atoms_dev(H, nchr, dcp.p, dq.p, s);
+    energy_dev(H, nchr, nullptr, nullptr, dx.p, soleng, couleng, s);
+  });
+}
+
+int tabi_run_dev(tabi_h h, int nspt, const double* sptpos_dev, const double* sptnrm_dev,
+                 int nface, const int* nvert_dev, int nchr, const double* chrpos_dev,
+                 const double* atmchr_dev, double* x_dev, double* stats, void* stream) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(nspt > 0 && nface > 0 && nchr > 0, TABI_ERR_ARG, "sizes must be positive");
+    TABI_REQUIRE(sptpos_dev && sptnrm_dev && nvert_dev && chrpos_dev && atmchr_dev,
+                 TABI_ERR_ARG, "null input");
+    set_device(H);
+    cudaStream_t s = pick(H, stream);
+    cudaStream_t keep = H.stream;
+    H.stream = s;
+    struct Restore {
+      Handle& H;
+      cudaStream_t k;
+      ~Restore() { H.stream = k; }
+    } restore{H, keep};
+    alloc_surface(H, nface);
+    pack_atoms_dev(H, nchr, chrpos_dev, atmchr_dev, s);
+    DBuf<double> b0, b;
+    b0.alloc(2 * (size_t)nface);
+    b.alloc(2 * (size_t)nface);
+    launch_form_matrix(H, nspt, sptpos_dev, sptnrm_dev, nface, nvert_dev, nchr, H.d_atoms.p,
+                       b0.p, s);
+    H.has_surface = true;
+    do_build(H, s);
+    { TABI_K(K_FORM, s); permute_b_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(H.d_perm.p, nface, b0.p, b.p); }
+    DBuf<double> xl;
+    double* x = x_dev;
+    if (!x) {
+      xl.alloc(2 * (size_t)nface);
+      x = xl.p;
+    }
+    TABI_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * 2 * nface, s));
+    int iter = 0, ierr = 0;
+    double err = 0.0, se = 0.0, ce = 0.0;
+    gmres_dev(H, b.p, x, &iter, &err, &ierr, nullptr, nullptr, s);
+    energy_dev(H, nchr, nullptr, nullptr, x, &se, &ce, s);
+    if (stats) {
+      stats[0] = iter;
+      stats[1] = err;
+      stats[2] = ierr;
+      stats[3] = se;
+      stats[4] = ce;
+      stats[5] = (double)H.tree.n_near_pairs;
+      stats[6] = (double)H.tree.n_far;
+      stats[7] = H.tree.nleaf;
+    }
+  });
+}
+
+int tabi_counts(tabi_h h, int64_t* near_pairs, int64_t* far_interactions) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(H.has_tree, TABI_ERR_STATE, "no tree");
+    if (near_pairs) *near_pairs = H.tree.n_near_pairs;
+    if (far_interactions) *far_interactions = H.tree.n_far;
+  });
+}
+
+int tabi_tree_nodes(tabi_h h, int* nnodes, int* ibeg, int* numpar, int* level, int* nchild,
+                    double* geo) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(H.has_tree, TABI_ERR_STATE, "no tree");
+    Tree& T = H.tree;
+    if (nnodes) *nnodes = T.nnodes;
+    if (!ibeg && !numpar && !level && !nchild && !geo) return;
+    // depth-first (creation) order of the reference
+    std::vector<int> order, stack = {0};
+    while (!stack.empty()) {
+      int c = stack.back();
+      stack.pop_back();
+      order.push_back(c);
+      for (int k = T.nchild[c] - 1; k >= 0; --k) stack.push_back(T.child0[c] + k);
+    }
+    for (size_t k = 0; k < order.size(); ++k) {
+      int c = order[k];
+      if (ibeg) ibeg[k] = T.ibeg[c] + 1;
+      if (numpar) numpar[k] = T.num[c];
+      if (level) level[k] = T.level[c];
+      if (nchild) nchild[k] = T.nchild[c];
+      if (geo) {
+        geo[4 * k] = T.mid[3 * c];
+        geo[4 * k + 1] = T.mid[3 * c + 1];
+        geo[4 * k + 2] = T.mid[3 * c + 2];
+        geo[4 * k + 3] = T.rad[c];
+      }
+    }
+  });
+}
+
+int tabi_profile_enable(tabi_h h, int enable) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    H.prof.reset();
+    H.prof.on = enable != 0;
+  });
+}
+
+int tabi_profile_read(tabi_h h, int kclass, double* ms, int64_t* launches) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(kclass >= -1 && kclass < K_NCLASS, TABI_ERR_ARG, "bad kernel class");
+    H.prof.resolve();
+    double t = 0.0;
+    int64_t l = 0;
+    for (int k = 0; k < K_NCLASS; ++k)
+      if (kclass == -1 || kclass == k) {
+        t += H.prof.ms[k];
+        l += H.prof.launches[k];
+      }
+    if (ms) *ms = t;
+    if (launches) *launches = l;
+  });
+}
+
+int tabi_profile_nclasses(void) { return K_NCLASS; }
+
+const char* tabi_profile_class_name(int kclass) {
+  static const char* names[K_NCLASS] = {"form_matrix", "tree", "lists",   "moments",
+                                        "far",         "near", "reduce",  "assemble",
+                                        "lu",          "solve", "vector", "energy"};
+  return (kclass >= 0 && kclass < K_NCLASS) ? names[kclass] : "all";
+}
+
+int tabi_probe_fp64_peak(double ms, double* flops) {
+  if (!flops) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    int dev = 0, nsm = 0;
+    TABI_CUDA(cudaGetDevice(&dev));
+    TABI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    DBuf<double> out;
+    out.alloc(1);
+    cudaEvent_t e0, e1;
+    TABI_CUDA(cudaEventCreate(&e0));
+    TABI_CUDA(cudaEventCreate(&e1));
+    int blocks = nsm * 8, threads = 256;
+    long iters = 64;
+    double t = 0.0;
+    for (int rep = 0; rep < 12; ++rep) {
+      TABI_CUDA(cudaEventRecord(e0));
+      fp64_peak_kernel<<<blocks, threads>>>(out.p, iters);
+      TABI_CUDA(cudaEventRecord(e1));
+      TABI_CUDA(cudaEventSynchronize(e1));
+      float f = 0;
+      TABI_CUDA(cudaEventElapsedTime(&f, e0, e1));
+      t = f;
+      if (t >= ms) break;
+      iters = (long)(iters * std::min(8.0, std::max(1.5, ms / std::max(t, 1e-3))));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    double fl = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    *flops = fl / (t * 1e-3);
+  });
+}
+
+}  // extern "C"

@@ -1,0 +1,262 @@
+// tabi_impl.cuh -- internal state and kernel declarations of libtabi_gpu.so.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/tabi_gpu.h"
+
+namespace tabi {
+
+constexpr double kPi = 3.141592653589793238462643383279;
+constexpr double kOneOver4Pi = 0.25 / 3.141592653589793238462643383279;
+constexpr int kMaxOrder = 8;
+constexpr int kMacMinPar = 40;   // treecode3d_pb.f:393 (numpar > 40)
+constexpr int kStack = 512;      // per-warp traversal stack entries
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define TABI_CUDA(call)                                                     \
+  do {                                                                      \
+    cudaError_t e_ = (call);                                                \
+    if (e_ != cudaSuccess)                                                  \
+      throw ::tabi::Error(e_ == cudaErrorMemoryAllocation ? TABI_ERR_NOMEM  \
+                                                          : TABI_ERR_CUDA,  \
+                          std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define TABI_REQUIRE(cond, code, msg)                   \
+  do {                                                  \
+    if (!(cond)) throw ::tabi::Error((code), (msg));    \
+  } while (0)
+
+// Device buffer owned by the handle (freed on reset / destroy).
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  void alloc(size_t count) {
+    if (count <= n && p) return;
+    release();
+    if (count == 0) return;
+    TABI_CUDA(cudaMalloc(&p, count * sizeof(T)));
+    n = count;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+  ~DBuf() { release(); }
+  DBuf() = default;
+  DBuf(const DBuf&) = delete;
+  DBuf& operator=(const DBuf&) = delete;
+  DBuf(DBuf&& o) noexcept : p(o.p), n(o.n) {
+    o.p = nullptr;
+    o.n = 0;
+  }
+  DBuf& operator=(DBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      p = o.p;
+      n = o.n;
+      o.p = nullptr;
+      o.n = 0;
+    }
+    return *this;
+  }
+};
+
+// Work item of the interaction kernels: node and a chunk of its entry list.
+struct WorkItem {
+  int node;
+  int start;  // offset into the node's entry list
+  int count;
+  int mslot;  // moment slot (far) or leaf ibeg (near)
+};
+
+struct Tree {
+  int n = 0;          // faces
+  int nnodes = 0;
+  int nleaf = 0;
+  int depth = 0;
+  // host mirror of the node table (BFS order: children of a node contiguous)
+  std::vector<int> ibeg, num, child0, nchild, level;
+  std::vector<double> mid, rad;  // mid 3 per node
+  std::vector<int> leaves;       // leaf node ids in tree order
+  // device node table
+  DBuf<int> d_ibeg, d_num, d_child0, d_nchild;
+  DBuf<double> d_mid, d_rad;
+  // interaction lists
+  int64_t n_near_pairs = 0, n_far = 0, n_slots = 0;
+  DBuf<int64_t> d_slot_off;    // n+1
+  DBuf<int2> d_far_ent;        // (target, slot) grouped by cluster
+  DBuf<int2> d_near_ent;       // (target, slot) grouped by leaf
+  std::vector<WorkItem> far_work, near_work;
+  DBuf<WorkItem> d_far_work, d_near_work;
+  int nmslot = 0;
+  std::vector<int> mslot_node;  // node id per moment slot
+  DBuf<int> d_mslot_node;
+  std::vector<int> mchunk_node, mchunk_start, mchunk_count;  // moment chunks
+  DBuf<int4> d_mchunks;  // (slot, node ibeg+start, count, chunk id)
+  std::vector<int> mslot_chunk0, mslot_nchunk;
+  DBuf<int2> d_mslot_chunks;
+  // preconditioner
+  std::vector<int64_t> blk_off;  // per leaf offset into the factor buffer
+  DBuf<double> d_lu;
+  DBuf<int> d_piv;               // 2n per leaf, offsets 2*ibeg
+  DBuf<int64_t> d_blk_off;
+  DBuf<int2> d_leaf_rng;         // (ibeg, n) per leaf
+  int max_leaf = 0;
+};
+
+// Kernel classes for the launch counters / event timers (tabi_profile_*).
+enum KClass {
+  K_FORM = 0, K_TREE, K_LISTS, K_MOMENTS, K_FAR, K_NEAR, K_REDUCE, K_ASSEMBLE, K_LU,
+  K_SOLVE, K_VEC, K_ENERGY, K_NCLASS
+};
+
+struct Handle;
+
+struct Prof {
+  bool on = false;
+  int64_t launches[K_NCLASS] = {};
+  double ms[K_NCLASS] = {};
+  struct Rec {
+    cudaEvent_t a, b;
+    int kind;
+  };
+  std::vector<Rec> pending;
+  std::vector<cudaEvent_t> pool;
+  cudaEvent_t get() {
+    if (!pool.empty()) {
+      cudaEvent_t e = pool.back();
+      pool.pop_back();
+      return e;
+    }
+    cudaEvent_t e;
+    cudaEventCreate(&e);
+    return e;
+  }
+  void resolve() {
+    for (auto& r : pending) {
+      float f = 0.f;
+      cudaEventSynchronize(r.b);
+      cudaEventElapsedTime(&f, r.a, r.b);
+      ms[r.kind] += f;
+      pool.push_back(r.a);
+      pool.push_back(r.b);
+    }
+    pending.clear();
+  }
+  void reset() {
+    resolve();
+    for (int k = 0; k < K_NCLASS; ++k) {
+      launches[k] = 0;
+      ms[k] = 0.0;
+    }
+  }
+  ~Prof() {
+    for (auto& r : pending) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    for (auto e : pool) cudaEventDestroy(e);
+  }
+};
+
+// Counts one kernel launch of class `kind` and, when profiling is on, times
+// it with events recorded on the launching stream around the launch.
+struct KScope {
+  Prof& P;
+  int kind;
+  cudaStream_t s;
+  cudaEvent_t a = nullptr;
+  KScope(Prof& p, int k, cudaStream_t st) : P(p), kind(k), s(st) {
+    P.launches[kind]++;
+    if (P.on) {
+      a = P.get();
+      cudaEventRecord(a, s);
+    }
+  }
+  ~KScope() {
+    if (P.on) {
+      cudaEvent_t b = P.get();
+      cudaEventRecord(b, s);
+      P.pending.push_back({a, b, kind});
+    }
+  }
+};
+#define TABI_K(kind, s) ::tabi::KScope _kscope_(H.prof, (kind), (s))
+
+struct Handle {
+  tabi_params prm{};
+  Prof prof;
+  std::string err;
+  cudaStream_t stream = nullptr;
+  int device = 0;
+  int n = 0;  // faces
+  bool has_surface = false, has_tree = false, has_precond = false;
+  // surface in the handle's current order (original before the tree, tree
+  // order after)
+  DBuf<double> d_x, d_y, d_z, d_nx, d_ny, d_nz, d_area;
+  DBuf<int> d_perm;  // tree slot -> original index
+  std::vector<int> h_perm;
+  Tree tree;
+  // matvec scratch
+  DBuf<double> d_mraw;    // moment partials
+  DBuf<double> d_mw;      // weighted moments, 16 x NT per slot
+  DBuf<double2> d_res;    // per-slot interaction results
+  DBuf<double> d_red;     // reduction scratch
+  DBuf<double> h_red_pinned_dummy;
+  double* h_pinned = nullptr;  // small pinned host scratch (64 doubles)
+  // GMRES workspace
+  DBuf<double> d_v, d_wk, d_dl, d_gz, d_r, d_b, d_xio, d_tmp;
+  DBuf<double> d_coef;
+  // energy scratch
+  DBuf<double> d_ptl;
+  DBuf<double> d_atoms;
+  // tree-build scratch
+  DBuf<double> d_tx, d_ty, d_tz;
+  DBuf<int> d_tperm;
+  DBuf<unsigned char> d_code;
+  DBuf<unsigned long long> d_bbox;
+  DBuf<int> d_hist, d_base;
+  DBuf<int4> d_chunks;
+  DBuf<int> d_cnt;
+  DBuf<int> d_err;
+};
+
+// ---- kernels / launchers (defined in the .cu files) ----
+// form_matrix / rhs / energy (rhs_energy.cu)
+void launch_form_matrix(Handle& H, int nspt, const double* sptpos, const double* sptnrm,
+                        int nface, const int* nvert, int nchr, const double* atoms4,
+                        double* d_b, cudaStream_t s);
+void launch_rhs(Handle& H, int nchr, const double* atoms4, double* d_b, cudaStream_t s);
+void energy_dev(Handle& H, int nchr, const double* chrpos, const double* atmchr, const double* x,
+                double* soleng, double* couleng, cudaStream_t s);
+// tree + lists (tree.cu)
+void build_tree(Handle& H, cudaStream_t s);
+void build_lists(Handle& H, cudaStream_t s);
+// matvec (matvec.cu)
+void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool check_zero);
+double asum_dev(Handle& H, const double* x, int n, cudaStream_t s);
+// preconditioner (precond.cu)
+void build_precond(Handle& H, cudaStream_t s);
+void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s);
+// gmres (gmres.cu)
+void gmres_dev(Handle& H, const double* b, double* x, int* iter, double* err, int* ierr,
+               double* hist, int* nhist, cudaStream_t s);
+double dot_dev(Handle& H, const double* a, const double* b, int n, cudaStream_t s);
+double nrm2_dev(Handle& H, const double* a, int n, cudaStream_t s);
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+}  // namespace tabi

@@ -1,0 +1,340 @@
+/*
+ * surfgen.c -- molecular surface generator writing MSMS-format .vert/.face.
+ *
+ * The reference shells out to the prebuilt third-party MSMS binary
+ * (readin.f90:200-202: "msms -if <f>.xyzr -prob 1.4 -de <den> -of <f>") and
+ * reads back <f>.vert / <f>.face (readin.f90:204-246).  That binary is not
+ * usable here, so this file provides a generator of our own with the same
+ * command line and the same output format:
+ *
+ *   surface:  Gaussian level set  rho(x) = sum_i exp(-B (|x-c_i|^2/r_i^2 - 1)),
+ *             surface rho = 1, where r_i = atomic radius (+ 0 probe: the probe
+ *             radius only sets the default blobbiness B, larger probes giving
+ *             smoother surfaces);
+ *   mesh:     surface nets on a uniform grid (one vertex per grid cell that
+ *             the surface crosses, one quad per crossed grid edge, each quad
+ *             split along its shorter diagonal), vertices projected onto the
+ *             level set by Newton steps, normals = -grad rho / |grad rho|
+ *             (outward, as in MSMS).
+ *   density:  grid spacing chosen for the requested vertices per A^2.
+ *
+ * It is an SES stand-in, not MSMS: surface parity with MSMS is not claimed.
+ * The solver consumes whatever .vert/.face it is given; the same files feed
+ * the GPU path and the CPU oracle.
+ */
+#include "surfgen.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+typedef struct {
+  int natm;
+  const double* xyzr; /* natm x 4 */
+  double blob;
+  double cut2_scale; /* cutoff radius^2 = r^2 * cut2_scale */
+  /* atom bins */
+  double lo[3], bin;
+  int nb[3];
+  int *bin_start, *bin_atoms;
+} field_t;
+
+static void field_init(field_t* F, int natm, const double* xyzr, double blob) {
+  F->natm = natm;
+  F->xyzr = xyzr;
+  F->blob = blob;
+  /* contribution below 1e-6 of the level is dropped */
+  F->cut2_scale = 1.0 + log(1e6) / blob;
+  double rmax = 0.0;
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < natm; ++i) {
+    for (int d = 0; d < 3; ++d) {
+      double v = xyzr[4 * i + d];
+      if (v < lo[d]) lo[d] = v;
+      if (v > hi[d]) hi[d] = v;
+    }
+    if (xyzr[4 * i + 3] > rmax) rmax = xyzr[4 * i + 3];
+  }
+  F->bin = rmax * sqrt(F->cut2_scale);
+  if (F->bin <= 0) F->bin = 1.0;
+  long nbt = 1;
+  for (int d = 0; d < 3; ++d) {
+    F->lo[d] = lo[d] - F->bin;
+    F->nb[d] = (int)((hi[d] - F->lo[d]) / F->bin) + 2;
+    nbt *= F->nb[d];
+  }
+  F->bin_start = (int*)calloc((size_t)nbt + 1, sizeof(int));
+  F->bin_atoms = (int*)malloc(sizeof(int) * (size_t)(natm > 0 ? natm : 1));
+  int* cell = (int*)malloc(sizeof(int) * (size_t)(natm > 0 ? natm : 1));
+  for (int i = 0; i < natm; ++i) {
+    int b[3];
+    for (int d = 0; d < 3; ++d) b[d] = (int)((xyzr[4 * i + d] - F->lo[d]) / F->bin);
+    cell[i] = (b[2] * F->nb[1] + b[1]) * F->nb[0] + b[0];
+    F->bin_start[cell[i] + 1]++;
+  }
+  for (long c = 0; c < nbt; ++c) F->bin_start[c + 1] += F->bin_start[c];
+  int* fill = (int*)calloc((size_t)nbt, sizeof(int));
+  for (int i = 0; i < natm; ++i)
+    F->bin_atoms[F->bin_start[cell[i]] + fill[cell[i]]++] = i;
+  free(fill);
+  free(cell);
+}
+
+static void field_free(field_t* F) {
+  free(F->bin_start);
+  free(F->bin_atoms);
+}
+
+/* rho(p) - 1 and its gradient */
+static double field_eval(const field_t* F, const double* p, double* grad) {
+  int b[3];
+  for (int d = 0; d < 3; ++d) b[d] = (int)floor((p[d] - F->lo[d]) / F->bin);
+  double rho = 0.0, g[3] = {0, 0, 0};
+  for (int bz = b[2] - 1; bz <= b[2] + 1; ++bz) {
+    if (bz < 0 || bz >= F->nb[2]) continue;
+    for (int by = b[1] - 1; by <= b[1] + 1; ++by) {
+      if (by < 0 || by >= F->nb[1]) continue;
+      for (int bx = b[0] - 1; bx <= b[0] + 1; ++bx) {
+        if (bx < 0 || bx >= F->nb[0]) continue;
+        int c = (bz * F->nb[1] + by) * F->nb[0] + bx;
+        for (int k = F->bin_start[c]; k < F->bin_start[c + 1]; ++k) {
+          const double* a = F->xyzr + 4 * F->bin_atoms[k];
+          double dx = p[0] - a[0], dy = p[1] - a[1], dz = p[2] - a[2];
+          double r2 = a[3] * a[3];
+          double d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 > r2 * F->cut2_scale) continue;
+          double e = exp(-F->blob * (d2 / r2 - 1.0));
+          rho += e;
+          double s = -2.0 * F->blob / r2 * e;
+          g[0] += s * dx;
+          g[1] += s * dy;
+          g[2] += s * dz;
+        }
+      }
+    }
+  }
+  if (grad) {
+    grad[0] = g[0];
+    grad[1] = g[1];
+    grad[2] = g[2];
+  }
+  return rho - 1.0;
+}
+
+typedef struct {
+  double* v;
+  int nv, cap;
+} vbuf;
+typedef struct {
+  int* f;
+  int nf, cap;
+} fbuf;
+
+static int vpush(vbuf* b, const double* p, const double* n) {
+  if (b->nv == b->cap) {
+    b->cap = b->cap ? 2 * b->cap : 4096;
+    b->v = (double*)realloc(b->v, sizeof(double) * 6 * (size_t)b->cap);
+  }
+  memcpy(b->v + 6 * (size_t)b->nv, p, 3 * sizeof(double));
+  memcpy(b->v + 6 * (size_t)b->nv + 3, n, 3 * sizeof(double));
+  return b->nv++;
+}
+static void fpush(fbuf* b, int a, int c, int d) {
+  if (b->nf == b->cap) {
+    b->cap = b->cap ? 2 * b->cap : 8192;
+    b->f = (int*)realloc(b->f, sizeof(int) * 3 * (size_t)b->cap);
+  }
+  b->f[3 * (size_t)b->nf + 0] = a;
+  b->f[3 * (size_t)b->nf + 1] = c;
+  b->f[3 * (size_t)b->nf + 2] = d;
+  b->nf++;
+}
+
+static double d2v(const double* v, int a, int b) {
+  const double* p = v + 6 * (size_t)a;
+  const double* q = v + 6 * (size_t)b;
+  double dx = p[0] - q[0], dy = p[1] - q[1], dz = p[2] - q[2];
+  return dx * dx + dy * dy + dz * dz;
+}
+
+/* quad a-b-c-d (cyclic) -> two triangles split on the shorter diagonal */
+static void quad(fbuf* F, const double* v, int a, int b, int c, int d) {
+  if (d2v(v, a, c) <= d2v(v, b, d)) {
+    fpush(F, a, b, c);
+    fpush(F, a, c, d);
+  } else {
+    fpush(F, a, b, d);
+    fpush(F, b, c, d);
+  }
+}
+
+int sg_gaussian_surface(int natm, const double* xyzr, double probe,
+                        double density, double blob, double** vert_out,
+                        int* nvert_out, int** face_out, int* nface_out,
+                        double* spacing_out) {
+  if (natm <= 0 || density <= 0) return -1;
+  if (blob <= 0) blob = 2.0 + 0.5 * probe; /* default blobbiness */
+  field_t F;
+  field_init(&F, natm, xyzr, blob);
+  /* surface nets give about 1.6 vertices per h^2 of surface */
+  double h = sqrt(1.6 / density);
+  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
+  for (int i = 0; i < natm; ++i)
+    for (int d = 0; d < 3; ++d) {
+      double r = xyzr[4 * i + 3] * sqrt(F.cut2_scale);
+      if (xyzr[4 * i + d] - r < lo[d]) lo[d] = xyzr[4 * i + d] - r;
+      if (xyzr[4 * i + d] + r > hi[d]) hi[d] = xyzr[4 * i + d] + r;
+    }
+  int n[3];
+  for (int d = 0; d < 3; ++d) {
+    lo[d] -= 2 * h;
+    n[d] = (int)ceil((hi[d] + 2 * h - lo[d]) / h) + 1;
+  }
+  size_t NG = (size_t)n[0] * n[1] * n[2];
+  double* f = (double*)malloc(sizeof(double) * NG);
+  for (size_t i = 0; i < NG; ++i) f[i] = -1.0;
+  /* splat atoms onto the grid within the cutoff */
+  for (int a = 0; a < natm; ++a) {
+    const double* c = xyzr + 4 * a;
+    double r2 = c[3] * c[3];
+    double rc = c[3] * sqrt(F.cut2_scale);
+    int i0[3], i1[3];
+    for (int d = 0; d < 3; ++d) {
+      i0[d] = (int)floor((c[d] - rc - lo[d]) / h);
+      i1[d] = (int)ceil((c[d] + rc - lo[d]) / h);
+      if (i0[d] < 0) i0[d] = 0;
+      if (i1[d] > n[d] - 1) i1[d] = n[d] - 1;
+    }
+    for (int k = i0[2]; k <= i1[2]; ++k) {
+      double dz = lo[2] + k * h - c[2];
+      for (int j = i0[1]; j <= i1[1]; ++j) {
+        double dy = lo[1] + j * h - c[1];
+        for (int i = i0[0]; i <= i1[0]; ++i) {
+          double dx = lo[0] + i * h - c[0];
+          double d2 = dx * dx + dy * dy + dz * dz;
+          if (d2 > r2 * F.cut2_scale) continue;
+          f[((size_t)k * n[1] + j) * n[0] + i] += exp(-blob * (d2 / r2 - 1.0));
+        }
+      }
+    }
+  }
+#define G(i, j, k) f[((size_t)(k) * n[1] + (j)) * n[0] + (i)]
+  int* cv = (int*)malloc(sizeof(int) * NG);
+  for (size_t i = 0; i < NG; ++i) cv[i] = -1;
+  vbuf V = {0};
+  static const int corner[8][3] = {{0, 0, 0}, {1, 0, 0}, {0, 1, 0}, {1, 1, 0},
+                                   {0, 0, 1}, {1, 0, 1}, {0, 1, 1}, {1, 1, 1}};
+  static const int edge[12][2] = {{0, 1}, {2, 3}, {4, 5}, {6, 7}, {0, 2}, {1, 3},
+                                  {4, 6}, {5, 7}, {0, 4}, {1, 5}, {2, 6}, {3, 7}};
+  for (int k = 0; k < n[2] - 1; ++k)
+    for (int j = 0; j < n[1] - 1; ++j)
+      for (int i = 0; i < n[0] - 1; ++i) {
+        double val[8];
+        int mask = 0;
+        for (int c = 0; c < 8; ++c) {
+          val[c] = G(i + corner[c][0], j + corner[c][1], k + corner[c][2]);
+          if (val[c] > 0) mask |= 1 << c;
+        }
+        if (mask == 0 || mask == 255) continue;
+        double p[3] = {0, 0, 0};
+        int cnt = 0;
+        for (int e = 0; e < 12; ++e) {
+          int a = edge[e][0], b = edge[e][1];
+          if (((mask >> a) & 1) == ((mask >> b) & 1)) continue;
+          double t = val[a] / (val[a] - val[b]);
+          for (int d = 0; d < 3; ++d)
+            p[d] += (corner[a][d] + t * (corner[b][d] - corner[a][d]));
+          cnt++;
+        }
+        for (int d = 0; d < 3; ++d) p[d] = lo[d] + h * ((d == 0 ? i : d == 1 ? j : k) + p[d] / cnt);
+        /* project onto rho = 1 (few Newton steps, step bounded by h) */
+        double g[3];
+        for (int it = 0; it < 4; ++it) {
+          double fv = field_eval(&F, p, g);
+          double gg = g[0] * g[0] + g[1] * g[1] + g[2] * g[2];
+          if (gg <= 0) break;
+          double s = fv / gg;
+          double step = fabs(s) * sqrt(gg);
+          if (step > 0.5 * h) s *= 0.5 * h / step;
+          for (int d = 0; d < 3; ++d) p[d] -= s * g[d];
+          if (step < 1e-9) break;
+        }
+        field_eval(&F, p, g);
+        double gn = sqrt(g[0] * g[0] + g[1] * g[1] + g[2] * g[2]);
+        double nrm[3] = {0, 0, 1};
+        if (gn > 0)
+          for (int d = 0; d < 3; ++d) nrm[d] = -g[d] / gn;
+        cv[((size_t)k * n[1] + j) * n[0] + i] = vpush(&V, p, nrm);
+      }
+#define CV(i, j, k) cv[((size_t)(k) * n[1] + (j)) * n[0] + (i)]
+  fbuf FB = {0};
+  for (int k = 1; k < n[2] - 1; ++k)
+    for (int j = 1; j < n[1] - 1; ++j)
+      for (int i = 1; i < n[0] - 1; ++i) {
+        int in0 = G(i, j, k) > 0;
+        /* x-edge (i,j,k)-(i+1,j,k): cells around it differ in j-1..j, k-1..k */
+        if (i < n[0] - 1 && in0 != (G(i + 1, j, k) > 0)) {
+          int a = CV(i, j - 1, k - 1), b = CV(i, j, k - 1), c = CV(i, j, k), d = CV(i, j - 1, k);
+          if (a >= 0 && b >= 0 && c >= 0 && d >= 0) {
+            if (in0) quad(&FB, V.v, a, b, c, d); else quad(&FB, V.v, d, c, b, a);
+          }
+        }
+        if (j < n[1] - 1 && in0 != (G(i, j + 1, k) > 0)) {
+          int a = CV(i - 1, j, k - 1), b = CV(i - 1, j, k), c = CV(i, j, k), d = CV(i, j, k - 1);
+          if (a >= 0 && b >= 0 && c >= 0 && d >= 0) {
+            if (in0) quad(&FB, V.v, a, b, c, d); else quad(&FB, V.v, d, c, b, a);
+          }
+        }
+        if (k < n[2] - 1 && in0 != (G(i, j, k + 1) > 0)) {
+          int a = CV(i - 1, j - 1, k), b = CV(i, j - 1, k), c = CV(i, j, k), d = CV(i - 1, j, k);
+          if (a >= 0 && b >= 0 && c >= 0 && d >= 0) {
+            if (in0) quad(&FB, V.v, a, b, c, d); else quad(&FB, V.v, d, c, b, a);
+          }
+        }
+      }
+#undef G
+#undef CV
+  free(f);
+  free(cv);
+  field_free(&F);
+  /* to 1-based indices like MSMS */
+  for (int i = 0; i < 3 * FB.nf; ++i) FB.f[i] += 1;
+  *vert_out = V.v;
+  *nvert_out = V.nv;
+  *face_out = FB.f;
+  *nface_out = FB.nf;
+  if (spacing_out) *spacing_out = h;
+  return 0;
+}
+
+void sg_free(void* p) { free(p); }
+
+int sg_write_msms(const char* prefix, int nvert, const double* vert,
+                  int nface, const int* face, int natm, double density,
+                  double probe) {
+  char path[4096];
+  snprintf(path, sizeof path, "%s.vert", prefix);
+  FILE* fv = fopen(path, "w");
+  if (!fv) return -1;
+  fprintf(fv, "# MSMS solvent excluded surface vertices for %s\n", prefix);
+  fprintf(fv, "#vertex #sphere density probe_r\n");
+  fprintf(fv, "%7d %7d %6.2f %4.2f\n", nvert, natm, density, probe);
+  for (int i = 0; i < nvert; ++i) {
+    const double* v = vert + 6 * (size_t)i;
+    fprintf(fv, "%9.3f %9.3f %9.3f %9.3f %9.3f %9.3f %7d %7d %2d\n", v[0], v[1],
+            v[2], v[3], v[4], v[5], 0, 1, 1);
+  }
+  fclose(fv);
+  snprintf(path, sizeof path, "%s.face", prefix);
+  FILE* ff = fopen(path, "w");
+  if (!ff) return -1;
+  fprintf(ff, "# MSMS solvent excluded surface faces for %s\n", prefix);
+  fprintf(ff, "#faces  #sphere density probe_r\n");
+  fprintf(ff, "%7d %7d %6.2f %4.2f\n", nface, natm, density, probe);
+  for (int i = 0; i < nface; ++i)
+    fprintf(ff, "%6d %6d %6d %2d %6d\n", face[3 * (size_t)i], face[3 * (size_t)i + 1],
+            face[3 * (size_t)i + 2], 1, 1);
+  fclose(ff);
+  return 0;
+}
