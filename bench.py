@@ -35,9 +35,18 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [os.path.join(ROOT, "tabi-pb_b200"), os.path.join(ROOT, "oracle")]
 
-WORKLOAD = dict(natm=2000, radius=18.0, min_sep=2.0, density=10.0, probe=1.4, seed=0,
-                order=3, theta=0.8, maxparnode=500, tol=1e-4, eps0=1.0, eps1=80.0, bulk=0.15)
-WORKLOAD_NAME = "globular-2000-atoms-18A-10vA2-p3-mac0.8-leaf500-fp64"
+WORKLOADS = {
+    # the benchmark configuration (see module docstring)
+    "globular": dict(natm=2000, radius=18.0, min_sep=2.0, density=10.0, probe=1.4, seed=0,
+                     order=3, theta=0.8, maxparnode=500, tol=1e-4, eps0=1.0, eps1=80.0,
+                     bulk=0.15, name="globular-2000-atoms-18A-10vA2-p3-mac0.8-leaf500-fp64"),
+    # a smaller molecule with the same settings, for profiler captures
+    "medium": dict(natm=600, radius=12.0, min_sep=2.0, density=10.0, probe=1.4, seed=0,
+                   order=3, theta=0.8, maxparnode=500, tol=1e-4, eps0=1.0, eps1=80.0,
+                   bulk=0.15, name="globular-600-atoms-12A-10vA2-p3-mac0.8-leaf500-fp64"),
+}
+WORKLOAD = WORKLOADS["globular"]
+WORKLOAD_NAME = WORKLOAD["name"]
 METRIC = "solves/s (TABI-PB solve at <=1e-4 dG error; plain FP64)"
 # GMRES iterations of this workload, from the parity-checked GPU run (the
 # oracle reproduces the GPU's iteration count; used to scale the CPU sample)
@@ -381,9 +390,13 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("gpu", "reference"), default="gpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--iters", type=int, default=12,
+    ap.add_argument("--iters", type=int, default=27,
                     help="GMRES iterations used to scale the reference-arm sample")
+    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="globular")
     args = ap.parse_args()
+    global WORKLOAD, WORKLOAD_NAME
+    WORKLOAD = WORKLOADS[args.workload]
+    WORKLOAD_NAME = WORKLOAD["name"]
     if args.impl == "reference":
         reference_arm(args)
     else:

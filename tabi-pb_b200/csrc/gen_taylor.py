@@ -12,8 +12,9 @@ This script emits, for each order P, a device function that
     the reference uses for its index pattern, so its value is the same),
   * walks the entries shell by shell (total degree 0, 1, ...), so that a value
     stays live for at most two further shells and the arrays live in registers,
-  * folds every a(m) into the 16 contraction sums as soon as it is known, with
-    the moments pre-weighted by the integer part of der_cof,
+  * folds every a(m) into the contraction sums as soon as it is known, with
+    the moments pre-weighted by the integer part of der_cof (the 16 index
+    sums fold into 8 accumulators, one per distinct target charge),
   * drops every b term for kappa = 0 (there b(0,0,0) = 1 is only ever
     multiplied by kappa = 0, and all other b vanish).
 Output: the two potentials of COMPP_TREE_PB before the 1/(4 pi) factor.
@@ -25,6 +26,15 @@ import sys
 
 KK = [(0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 0, 0), (0, 1, 0), (0, 0, 1), (2, 0, 0),
       (1, 1, 0), (1, 0, 1), (1, 1, 0), (0, 2, 0), (0, 1, 1), (1, 0, 1), (0, 1, 1), (0, 0, 2)]
+
+
+# The 16 contraction sums fold into 8 accumulators per kappa: indices with the
+# same target charge (pb_kernel, main.f90:671-690) share one: idx 1 (charge 1),
+# idx 2-4 (charge 1), idx 5/6/7 (n_x/n_y/n_z), idx 8+3i+j (n_j) for j = x,y,z.
+BARRIER = False
+ACC_NAMES = ["P", "G", "F0", "F1", "F2", "Hx", "Hy", "Hz"]
+ACC_OF = ["P", "G", "G", "G", "F0", "F1", "F2", "Hx", "Hy", "Hz", "Hx", "Hy", "Hz", "Hx", "Hy",
+          "Hz"]
 
 
 def terms(p):
@@ -184,10 +194,12 @@ def gen_pass(p, kap, pre):
         for n in range(2, top + 1):
             out.append(f"    const T cf1n_{n} = T({lit(1.0 / n)}) * kappa;")
         out.append("    const T ex = exp(-kappa * dist);")
-    for idx in range(16):
-        out.append(f"    T {pre}{idx} = T(0);")
+    for name in ACC_NAMES:
+        out.append(f"    T {pre}{name} = T(0);")
     out.append("    {")
     for n in range(top + 1):
+        if n > 0 and BARRIER:
+            out.append("    asm volatile(\"\" ::: \"memory\");  // keep moment loads in their shell")
         for k3 in range(n + 1):
             for k2 in range(n - k3 + 1):
                 k1 = n - k3 - k2
@@ -199,39 +211,45 @@ def gen_pass(p, kap, pre):
                     m = (k1 - kk[0], k2 - kk[1], k3 - kk[2])
                     if min(m) < 0 or sum(m) > p:
                         continue
-                    out.append(f"    {pre}{idx} = fma(a_{k1}_{k2}_{k3}, Mw[{idx * nt + tindex[m]}], {pre}{idx});")
+                    acc = pre + ACC_OF[idx]
+                    out.append(f"    {acc} = fma(a_{k1}_{k2}_{k3}, Mw[{idx * nt + tindex[m]}], {acc});")
     out.append("    }")
     return out
 
 
 def gen_order(p):
+    """Two passes per order, each its own non-inlined function: kept apart, each
+    pass is register-allocated on its own (about 140 registers, no spills, at
+    p = 3); inlined together the scheduler interleaves them and spills."""
     nt = len(terms(p))
-    L = [f"// ---- order {p}: {nt} moment terms per index, recurrence to degree {p + 2}",
-         "template <typename T>",
-         f"__device__ __forceinline__ void far_eval_p{p}(T dx, T dy, T dz, T kappa, const T* __restrict__ Mw,",
-         "                                               T n0, T n1, T n2, T eps, T inv_eps,",
-         "                                               T& out1, T& out2) {",
-         "  const T ddx = T(2) * dx, ddy = T(2) * dy, ddz = T(2) * dz;",
-         "  T dist = dx * dx + dy * dy + dz * dz;",
-         "  const T fac = T(1) / dist;",
-         "  dist = sqrt(dist);",
-         "  T P0, G0, F00, F01, F02, H0, P1, G1, F10, F11, F12, H1;",
-         "  {"]
-    L += gen_pass(p, False, "u")
-    L += ["    P0 = u0; G0 = u1 + u2 + u3; F00 = u4; F01 = u5; F02 = u6;",
-          "    H0 = n0 * (u7 + u10 + u13) + n1 * (u8 + u11 + u14) + n2 * (u9 + u12 + u15);",
-          "  }",
-          "  {",
-          "    const T kappax = kappa * dx, kappay = kappa * dy, kappaz = kappa * dz;"]
-    L += gen_pass(p, True, "v")
-    L += ["    P1 = v0; G1 = v1 + v2 + v3; F10 = v4; F11 = v5; F12 = v6;",
-          "    H1 = n0 * (v7 + v10 + v13) + n1 * (v8 + v11 + v14) + n2 * (v9 + v12 + v15);",
-          "  }",
-          "  const T nF0 = n0 * F00 + n1 * F01 + n2 * F02;",
-          "  const T nF1 = n0 * F10 + n1 * F11 + n2 * F12;",
+    L = [f"// ---- order {p}: {nt} moment terms per index, recurrence to degree {p + 2}"]
+    for kap, pre, fn in ((False, "u", "far_pass0"), (True, "v", "far_pass1")):
+        L += ["template <typename T>",
+              f"__device__ __noinline__ TabiFar4<T> {fn}_p{p}(T dx, T dy, T dz, T kappa,",
+              "                                             const T* __restrict__ Mw, T n0, T n1, T n2) {",
+              "  const T ddx = T(2) * dx, ddy = T(2) * dy, ddz = T(2) * dz;",
+              "  T dist = dx * dx + dy * dy + dz * dz;",
+              "  const T fac = T(1) / dist;",
+              "  dist = sqrt(dist);"]
+        if kap:
+            L.append("  const T kappax = kappa * dx, kappay = kappa * dy, kappaz = kappa * dz;")
+        L += gen_pass(p, kap, pre)
+        L += [f"  TabiFar4<T> r;",
+              f"  r.P = {pre}P;",
+              f"  r.G = {pre}G;",
+              f"  r.nF = n0 * {pre}F0 + n1 * {pre}F1 + n2 * {pre}F2;",
+              f"  r.nH = n0 * {pre}Hx + n1 * {pre}Hy + n2 * {pre}Hz;",
+              "  return r;",
+              "}", ""]
+    L += ["template <typename T>",
+          f"__device__ __forceinline__ void far_eval_p{p}(T dx, T dy, T dz, T kappa, const T* __restrict__ Mw,",
+          "                                               T n0, T n1, T n2, T eps, T inv_eps,",
+          "                                               T& out1, T& out2) {",
+          f"  const TabiFar4<T> c = far_pass0_p{p}<T>(dx, dy, dz, T(0), Mw, n0, n1, n2);",
+          f"  const TabiFar4<T> y = far_pass1_p{p}<T>(dx, dy, dz, kappa, Mw, n0, n1, n2);",
           "  // COMPP_TREE_PB :479-485 (before the 1/(4 pi) of der_cof)",
-          "  out1 = (P0 - P1) + (eps * G1 - G0);",
-          "  out2 = -(nF0 - nF1 * inv_eps) + (H1 - H0);",
+          "  out1 = (c.P - y.P) + (eps * y.G - c.G);",
+          "  out2 = -(c.nF - y.nF * inv_eps) + (y.nH - c.nH);",
           "}", ""]
     return L
 
@@ -250,6 +268,12 @@ def main():
                  + ", ".join("{%d,%d,%d}" % t for t in tl) + "};")
     L.append("")
     L.append("__host__ __device__ constexpr int tabi_nterms(int p) { return (p + 1) * (p + 2) * (p + 3) / 6; }")
+    L.append("")
+    L.append("// Per-pass results: P (index 1), G (2-4), n.F (5-7), n.H (8-16).")
+    L.append("template <typename T>")
+    L.append("struct TabiFar4 {")
+    L.append("  T P, G, nF, nH;")
+    L.append("};")
     L.append("")
     for p in range(1, maxp + 1):
         L += gen_order(p)

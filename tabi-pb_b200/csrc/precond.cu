@@ -12,8 +12,8 @@
 // testing ILAENV, is the unblocked recursive DGETRF2: partial pivoting on the
 // largest |a|, first index on ties) and DGETRS, on EVERY call.  The block
 // never changes, so here it is assembled and factored once per tree
-// (right-looking LU with partial pivoting, the same pivot rule; one CTA per
-// leaf) and every apply is a blocked forward/back substitution.
+// (right-looking LU with partial pivoting, the same pivot rule, batched over
+// all leaves) and every apply is a blocked forward/back substitution.
 #include <algorithm>
 
 #include "bie_kernels.cuh"
@@ -77,15 +77,19 @@ __device__ __forceinline__ void argmax_merge(double& v, int& i, double v2, int i
   }
 }
 
-// Right-looking blocked LU with partial pivoting of one leaf block per CTA.
+// Right-looking blocked LU with partial pivoting of one leaf block per CTA,
+// panel in global memory (used for blocks too large for the shared-memory
+// panel of the batched kernels).
 __global__ void __launch_bounds__(kLuThreads) lu_kernel(const int2* __restrict__ leaf_rng,
                                                         const int64_t* __restrict__ blk_off,
                                                         double* __restrict__ lu,
                                                         int* __restrict__ piv,
-                                                        int* __restrict__ info) {
+                                                        int* __restrict__ info,
+                                                        int skip_max_m) {
   int leaf = blockIdx.x;
   int2 lr = leaf_rng[leaf];
   int m = 2 * lr.y;
+  if (m <= skip_max_m) return;  // factored by the batched kernels
   double* A = lu + blk_off[leaf];
   int* ip = piv + 2 * lr.x;
   __shared__ double s_v[kLuThreads / 32];
@@ -231,15 +235,251 @@ __global__ void __launch_bounds__(kLuThreads) lu_kernel(const int2* __restrict__
   if (tid == 0) info[leaf] = my_info;
 }
 
-constexpr int kSolveThreads = 256;
 
-// Forward/back substitution with the factored block (DGETRS 'N').
-__global__ void __launch_bounds__(kSolveThreads) solve_kernel(
+// Batched, level-synchronous right-looking LU with partial pivoting for all
+// leaf blocks of order m <= kPanelMaxM at once.  Panel step s (k0 = 16 s) is
+// two launches over every block that still has columns left:
+//   lu_panel_kernel   one CTA per block: the 16-column panel (rows k0..m-1)
+//                     in shared memory -- pivot search (largest |a|, first
+//                     index on ties, as IDAMAX), row swap, scaling, rank-1
+//                     updates -- written back with its pivots;
+//   lu_update_kernel  one CTA per 128-column strip: the panel's row swaps,
+//                     then for strips right of the panel U12 = L11^{-1} A12 and
+//                     A22 -= L21 U12 (64 x 128 tiles, 4 x 8 per thread); strips
+//                     left of the panel only take the swaps (LAPACK applies
+//                     every pivot to the L columns too).
+// The trailing updates of all blocks run concurrently across the GPU.
+constexpr int kBP = 16;            // panel width
+constexpr int kPanelMaxM = 1536;   // panel of 1536 x 16 doubles = 192 KB of smem
+constexpr int kPT = 256;           // panel kernel threads
+constexpr int kUT = 256;           // update kernel threads
+constexpr int kUC = 128;           // strip width
+constexpr int kUR = 64;            // row tile of the update
+
+__global__ void __launch_bounds__(kPT) lu_panel_kernel(const int* __restrict__ items, int k0,
+                                                       const int2* __restrict__ leaf_rng,
+                                                       const int64_t* __restrict__ blk_off,
+                                                       double* __restrict__ lu,
+                                                       int* __restrict__ piv,
+                                                       int* __restrict__ info) {
+  extern __shared__ double P[];
+  __shared__ double s_v[kPT / 32];
+  __shared__ int s_i[kPT / 32];
+  __shared__ int s_p;
+  const int leaf = items[blockIdx.x];
+  const int2 lr = leaf_rng[leaf];
+  const int m = 2 * lr.y;
+  const int nb = min(kBP, m - k0), mr = m - k0;
+  double* A = lu + blk_off[leaf];
+  int* ip = piv + 2 * lr.x;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int q = tid; q < nb * mr; q += kPT) {
+    int c = q / mr, r = q - c * mr;
+    P[q] = A[(size_t)(k0 + c) * m + k0 + r];
+  }
+  __syncthreads();
+  for (int j = 0; j < nb; ++j) {
+    double* col = P + (size_t)j * mr;
+    double bv = -1.0;
+    int bi = mr;
+    for (int i = j + tid; i < mr; i += kPT) argmax_merge(bv, bi, fabs(col[i]), i);
+    for (int o = 16; o > 0; o >>= 1) {
+      double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+      int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+      argmax_merge(bv, bi, v2, i2);
+    }
+    if (lane == 0) {
+      s_v[warp] = bv;
+      s_i[warp] = bi;
+    }
+    __syncthreads();
+    if (warp == 0) {
+      double v = (lane < kPT / 32) ? s_v[lane] : -1.0;
+      int i = (lane < kPT / 32) ? s_i[lane] : mr;
+      for (int o = 16; o > 0; o >>= 1) {
+        double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        int i2 = __shfl_xor_sync(0xffffffffu, i, o);
+        argmax_merge(v, i, v2, i2);
+      }
+      if (lane == 0) s_p = i;
+    }
+    __syncthreads();
+    int p = s_p;
+    const double pv = col[p];
+    if (pv == 0.0) {  // DGETRF2: INFO set, no swap, no scaling
+      if (tid == 0) {
+        atomicCAS(&info[leaf], 0, k0 + j + 1);
+        ip[k0 + j] = k0 + j + 1;
+      }
+      __syncthreads();
+      continue;
+    }
+    if (tid == 0) ip[k0 + j] = k0 + p + 1;  // 1-based, like LAPACK
+    if (p != j && tid < nb) {
+      double* cc = P + (size_t)tid * mr;
+      double t = cc[j];
+      cc[j] = cc[p];
+      cc[p] = t;
+    }
+    __syncthreads();
+    const double pk = col[j];
+    const bool recip = fabs(pk) >= 2.2250738585072014e-308;
+    const double rcp = 1.0 / pk;
+    for (int i = j + 1 + tid; i < mr; i += kPT) {
+      double l = recip ? col[i] * rcp : col[i] / pk;
+      col[i] = l;
+      for (int c = j + 1; c < nb; ++c) {
+        double* cc = P + (size_t)c * mr;
+        cc[i] = fma(-l, cc[j], cc[i]);
+      }
+    }
+    __syncthreads();
+  }
+  for (int q = tid; q < nb * mr; q += kPT) {
+    int c = q / mr, r = q - c * mr;
+    A[(size_t)(k0 + c) * m + k0 + r] = P[q];
+  }
+}
+
+// item = (leaf, c0, c1): columns [c0, c1) of the leaf block
+__global__ void __launch_bounds__(kUT) lu_update_kernel(const int3* __restrict__ items, int k0,
+                                                        const int2* __restrict__ leaf_rng,
+                                                        const int64_t* __restrict__ blk_off,
+                                                        double* __restrict__ lu,
+                                                        const int* __restrict__ piv) {
+  __shared__ double sL11[kBP][kBP + 1];
+  __shared__ double sU[kBP][kUC];
+  __shared__ double sL[kUR][kBP + 1];
+  __shared__ int s_rows[2 * kBP], s_src[2 * kBP];
+  __shared__ int s_nr;
+  const int3 it = items[blockIdx.x];
+  const int leaf = it.x, c0 = it.y, c1 = it.z;
+  const int2 lr = leaf_rng[leaf];
+  const int m = 2 * lr.y;
+  const int nb = min(kBP, m - k0);
+  double* A = lu + blk_off[leaf];
+  const int* ip = piv + 2 * lr.x;
+  const int tid = threadIdx.x;
+  const int ncol = c1 - c0;
+  // rows touched by the panel's swaps and, for each, the row its value comes from
+  if (tid == 0) {
+    int nr = 0;
+    for (int j = 0; j < nb; ++j) s_rows[nr++] = k0 + j;
+    for (int j = 0; j < nb; ++j) {
+      int p = ip[k0 + j] - 1;
+      bool have = false;
+      for (int q = 0; q < nr; ++q) have |= (s_rows[q] == p);
+      if (!have) s_rows[nr++] = p;
+    }
+    for (int q = 0; q < nr; ++q) s_src[q] = s_rows[q];
+    for (int j = 0; j < nb; ++j) {  // content[] of the rows after each swap, in order
+      int p = ip[k0 + j] - 1, a = -1, b = -1;
+      for (int q = 0; q < nr; ++q) {
+        if (s_rows[q] == k0 + j) a = q;
+        if (s_rows[q] == p) b = q;
+      }
+      int t = s_src[a];
+      s_src[a] = s_src[b];
+      s_src[b] = t;
+    }
+    s_nr = nr;
+  }
+  __syncthreads();
+  const int nr = s_nr;
+  if (tid < ncol) {
+    double* cc = A + (size_t)(c0 + tid) * m;
+    double v[2 * kBP];
+#pragma unroll
+    for (int q = 0; q < 2 * kBP; ++q)
+      if (q < nr) v[q] = cc[s_src[q]];
+#pragma unroll
+    for (int q = 0; q < 2 * kBP; ++q)
+      if (q < nr) cc[s_rows[q]] = v[q];
+  }
+  if (c1 <= k0) return;  // strip left of the panel: swaps only
+  for (int q = tid; q < nb * nb; q += kUT) {
+    int c = q / nb, r = q - c * nb;
+    sL11[r][c] = A[(size_t)(k0 + c) * m + k0 + r];
+  }
+  __syncthreads();
+  // U12 = L11^{-1} A12 (unit lower), one column per thread
+  if (tid < ncol) {
+    double* cc = A + (size_t)(c0 + tid) * m;
+    double x[kBP];
+#pragma unroll
+    for (int r = 0; r < kBP; ++r) x[r] = (r < nb) ? cc[k0 + r] : 0.0;
+#pragma unroll
+    for (int r = 1; r < kBP; ++r) {
+      double acc = x[r];
+#pragma unroll
+      for (int q = 0; q < kBP; ++q)
+        if (q < r) acc = fma(-sL11[r][q], x[q], acc);
+      x[r] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < kBP; ++r) {
+      if (r < nb) cc[k0 + r] = x[r];
+      sU[r][tid] = (r < nb) ? x[r] : 0.0;
+    }
+  } else if (tid < kUC) {
+#pragma unroll
+    for (int r = 0; r < kBP; ++r) sU[r][tid] = 0.0;
+  }
+  // A22 -= L21 U12
+  const int tr = tid & 15, tc = tid >> 4;
+  for (int r0 = k0 + nb; r0 < m; r0 += kUR) {
+    __syncthreads();
+    for (int q = tid; q < kUR * kBP; q += kUT) {
+      int k = q / kUR, rr = q - k * kUR;
+      int gr = r0 + rr;
+      sL[rr][k] = (gr < m && k < nb) ? A[(size_t)(k0 + k) * m + gr] : 0.0;
+    }
+    __syncthreads();
+    double acc[4][8];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+#pragma unroll
+    for (int k = 0; k < kBP; ++k) {
+      double lv[4], uv[8];
+#pragma unroll
+      for (int a = 0; a < 4; ++a) lv[a] = sL[tr + 16 * a][k];
+#pragma unroll
+      for (int b = 0; b < 8; ++b) uv[b] = sU[k][tc + 16 * b];
+#pragma unroll
+      for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 8; ++b) acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
+    }
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+      int c = tc + 16 * b;
+      if (c >= ncol) continue;
+      double* cc = A + (size_t)(c0 + c) * m;
+#pragma unroll
+      for (int a = 0; a < 4; ++a) {
+        int gr = r0 + tr + 16 * a;
+        if (gr < m) cc[gr] -= acc[a][b];
+      }
+    }
+  }
+}
+
+// Forward/back substitution with the factored block (DGETRS 'N'): 32-row
+// blocks; the diagonal 32 x 32 triangle is staged in shared memory and solved
+// by one warp, the rows below (above) are updated with a 32-wide GEMV by all
+// threads.  Large blocks run with 1024 threads so that each of the m/16
+// sequential block steps is short; leaf_list selects the leaves of a launch.
+template <int NT>
+__global__ void __launch_bounds__(NT) solve_kernel(
     const int2* __restrict__ leaf_rng, const int64_t* __restrict__ blk_off,
-    const double* __restrict__ lu, const int* __restrict__ piv, int N,
-    const double* __restrict__ r, double* __restrict__ z) {
+    const int* __restrict__ leaf_list, const double* __restrict__ lu,
+    const int* __restrict__ piv, int N, const double* __restrict__ r,
+    double* __restrict__ z) {
   extern __shared__ double xs[];
-  int leaf = blockIdx.x;
+  __shared__ double D[32][33];
+  int leaf = leaf_list[blockIdx.x];
   int2 lr = leaf_rng[leaf];
   int n = lr.y, m = 2 * n, ib = lr.x;
   const double* A = lu + blk_off[leaf];
@@ -259,22 +499,28 @@ __global__ void __launch_bounds__(kSolveThreads) solve_kernel(
         xs[p] = t;
       }
     }
-  __syncthreads();
   // L y = P r (unit lower)
   for (int k0 = 0; k0 < m; k0 += 32) {
     int nb = min(32, m - k0);
+    for (int q = tid; q < nb * nb; q += blockDim.x) {
+      int c = q / nb, rr = q - c * nb;
+      D[rr][c] = A[(size_t)(k0 + c) * m + k0 + rr];
+    }
+    __syncthreads();
     if (warp == 0) {
       double v = (lane < nb) ? xs[k0 + lane] : 0.0;
       for (int kk = 0; kk < nb; ++kk) {
         double xk = __shfl_sync(0xffffffffu, v, kk);
-        if (lane > kk && lane < nb) v = fma(-A[(size_t)(k0 + kk) * m + k0 + lane], xk, v);
+        if (lane > kk && lane < nb) v = fma(-D[lane][kk], xk, v);
       }
       if (lane < nb) xs[k0 + lane] = v;
     }
     __syncthreads();
     for (int i = k0 + nb + tid; i < m; i += blockDim.x) {
       double s = xs[i];
-      for (int q = 0; q < nb; ++q) s = fma(-A[(size_t)(k0 + q) * m + i], xs[k0 + q], s);
+      const double* a = A + (size_t)k0 * m + i;
+#pragma unroll 8
+      for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], xs[k0 + q], s);
       xs[i] = s;
     }
     __syncthreads();
@@ -283,19 +529,26 @@ __global__ void __launch_bounds__(kSolveThreads) solve_kernel(
   for (int kend = m; kend > 0; kend -= 32) {
     int k0 = max(0, kend - 32);
     int nb = kend - k0;
+    for (int q = tid; q < nb * nb; q += blockDim.x) {
+      int c = q / nb, rr = q - c * nb;
+      D[rr][c] = A[(size_t)(k0 + c) * m + k0 + rr];
+    }
+    __syncthreads();
     if (warp == 0) {
       double v = (lane < nb) ? xs[k0 + lane] : 0.0;
       for (int kk = nb - 1; kk >= 0; --kk) {
-        if (lane == kk) v = v / A[(size_t)(k0 + kk) * m + k0 + kk];
+        if (lane == kk) v = v / D[kk][kk];
         double xk = __shfl_sync(0xffffffffu, v, kk);
-        if (lane < kk) v = fma(-A[(size_t)(k0 + kk) * m + k0 + lane], xk, v);
+        if (lane < kk) v = fma(-D[lane][kk], xk, v);
       }
       if (lane < nb) xs[k0 + lane] = v;
     }
     __syncthreads();
     for (int i = tid; i < k0; i += blockDim.x) {
       double s = xs[i];
-      for (int q = 0; q < nb; ++q) s = fma(-A[(size_t)(k0 + q) * m + i], xs[k0 + q], s);
+      const double* a = A + (size_t)k0 * m + i;
+#pragma unroll 8
+      for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], xs[k0 + q], s);
       xs[i] = s;
     }
     __syncthreads();
@@ -336,9 +589,9 @@ void build_precond(Handle& H, cudaStream_t s) {
   T.d_piv.alloc(2 * (size_t)H.n);
   T.d_blk_off.alloc(nl);
   T.d_leaf_rng.alloc(nl);
-  DBuf<int2> d_tiles;
+  DBuf<int2>& d_tiles = H.pc_tiles;
   d_tiles.alloc(tiles.size());
-  DBuf<int> d_info;
+  DBuf<int>& d_info = H.pc_info;
   d_info.alloc(nl);
   TABI_CUDA(cudaMemcpyAsync(T.d_blk_off.p, T.blk_off.data(), sizeof(int64_t) * nl,
                             cudaMemcpyHostToDevice, s));
@@ -351,8 +604,76 @@ void build_precond(Handle& H, cudaStream_t s) {
                                                     H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p,
                                                     H.d_ny.p, H.d_nz.p, H.d_area.p,
                                                     H.prm.kappa, eps, T.d_lu.p); }
-  { TABI_K(K_LU, s); lu_kernel<<<nl, kLuThreads, 0, s>>>(T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
-                                      d_info.p); }
+  TABI_CUDA(cudaMemsetAsync(d_info.p, 0, sizeof(int) * nl, s));
+  {
+    // batched LU for blocks with m <= kPanelMaxM; the global-memory kernel for
+    // larger ones
+    int mmax = 0;
+    bool any_big = false;
+    for (int l = 0; l < nl; ++l) {
+      int m = 2 * rng[l].y;
+      if (m <= kPanelMaxM) mmax = std::max(mmax, m);
+      else any_big = true;
+    }
+    const int nsteps = (mmax + kBP - 1) / kBP;
+    std::vector<int> order(nl);
+    for (int l = 0; l < nl; ++l) order[l] = l;
+    std::sort(order.begin(), order.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
+    std::vector<int> pitems;
+    std::vector<int3> uitems;
+    std::vector<int> poff(nsteps + 1), uoff(nsteps + 1);
+    for (int st = 0; st < nsteps; ++st) {
+      const int k0 = st * kBP;
+      poff[st] = (int)pitems.size();
+      uoff[st] = (int)uitems.size();
+      for (int l : order) {
+        const int m = 2 * rng[l].y;
+        if (m > kPanelMaxM || m <= k0) continue;
+        pitems.push_back(l);
+        const int nb = std::min(kBP, m - k0);
+        for (int c0 = 0; c0 < k0; c0 += kUC) uitems.push_back(make_int3(l, c0, std::min(c0 + kUC, k0)));
+        for (int c0 = k0 + nb; c0 < m; c0 += kUC)
+          uitems.push_back(make_int3(l, c0, std::min(c0 + kUC, m)));
+      }
+    }
+    poff[nsteps] = (int)pitems.size();
+    uoff[nsteps] = (int)uitems.size();
+    H.pc_list.alloc(std::max<size_t>(pitems.size(), 1));
+    H.pc_items.alloc(std::max<size_t>(uitems.size(), 1));
+    if (!pitems.empty())
+      TABI_CUDA(cudaMemcpyAsync(H.pc_list.p, pitems.data(), sizeof(int) * pitems.size(),
+                                cudaMemcpyHostToDevice, s));
+    if (!uitems.empty())
+      TABI_CUDA(cudaMemcpyAsync(H.pc_items.p, uitems.data(), sizeof(int3) * uitems.size(),
+                                cudaMemcpyHostToDevice, s));
+    if (nsteps > 0) {
+      size_t smem = sizeof(double) * (size_t)mmax * kBP;
+      TABI_CUDA(cudaFuncSetAttribute(lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)std::max<size_t>(smem, 48 * 1024)));
+    }
+    for (int st = 0; st < nsteps; ++st) {
+      const int k0 = st * kBP;
+      const int np = poff[st + 1] - poff[st], nu = uoff[st + 1] - uoff[st];
+      // panel rows: the largest block still active at this step
+      const int mr = 2 * rng[pitems[poff[st]]].y - k0;
+      if (np > 0) {
+        TABI_K(K_LU, s);
+        lu_panel_kernel<<<np, kPT, sizeof(double) * (size_t)mr * kBP, s>>>(
+            H.pc_list.p + poff[st], k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
+            d_info.p);
+      }
+      if (nu > 0) {
+        TABI_K(K_LU, s);
+        lu_update_kernel<<<nu, kUT, 0, s>>>(H.pc_items.p + uoff[st], k0, T.d_leaf_rng.p,
+                                            T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
+      }
+    }
+    if (any_big) {
+      TABI_K(K_LU, s);
+      lu_kernel<<<nl, kLuThreads, 0, s>>>(T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
+                                          d_info.p, kPanelMaxM);
+    }
+  }
   std::vector<int> info(nl);
   TABI_CUDA(cudaMemcpyAsync(info.data(), d_info.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, s));
   TABI_CUDA(cudaStreamSynchronize(s));
@@ -361,6 +682,19 @@ void build_precond(Handle& H, cudaStream_t s) {
       throw Error(TABI_ERR_SINGULAR, "leaf block " + std::to_string(l) +
                                          " is singular (DGETRF info " +
                                          std::to_string(info[l]) + ")");
+  // apply lists: blocks of order > 256 (largest first) get 1024 threads
+  {
+    std::vector<int> big, small;
+    for (int l = 0; l < nl; ++l) (2 * rng[l].y > 256 ? big : small).push_back(l);
+    std::sort(big.begin(), big.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
+    T.n_solve_big = (int)big.size();
+    T.n_solve_small = (int)small.size();
+    big.insert(big.end(), small.begin(), small.end());
+    T.d_solve_list.alloc(std::max<size_t>(big.size(), 1));
+    TABI_CUDA(cudaMemcpyAsync(T.d_solve_list.p, big.data(), sizeof(int) * big.size(),
+                              cudaMemcpyHostToDevice, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+  }
   H.has_precond = true;
 }
 
@@ -376,11 +710,24 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
   }
   size_t smem = sizeof(double) * 2 * (size_t)T.max_leaf;
   TABI_REQUIRE(smem <= 200 * 1024, TABI_ERR_LIMIT, "leaf too large for the block solve");
-  if (smem > 48 * 1024)
-    TABI_CUDA(cudaFuncSetAttribute(solve_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)smem));
-  { TABI_K(K_SOLVE, s); solve_kernel<<<T.nleaf, kSolveThreads, smem, s>>>(T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p,
-                                                    T.d_piv.p, n, r, z); }
+  if (smem > 48 * 1024) {
+    TABI_CUDA(cudaFuncSetAttribute(solve_kernel<256>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    TABI_CUDA(cudaFuncSetAttribute(solve_kernel<1024>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  }
+  if (T.n_solve_big > 0) {
+    TABI_K(K_SOLVE, s);
+    solve_kernel<1024><<<T.n_solve_big, 1024, smem, s>>>(T.d_leaf_rng.p, T.d_blk_off.p,
+                                                         T.d_solve_list.p, T.d_lu.p, T.d_piv.p,
+                                                         n, r, z);
+  }
+  if (T.n_solve_small > 0) {
+    TABI_K(K_SOLVE, s);
+    solve_kernel<256><<<T.n_solve_small, 256, smem, s>>>(T.d_leaf_rng.p, T.d_blk_off.p,
+                                                         T.d_solve_list.p + T.n_solve_big,
+                                                         T.d_lu.p, T.d_piv.p, n, r, z);
+  }
   TABI_CUDA(cudaGetLastError());
 }
 

@@ -1,7 +1,10 @@
 // tabi_api.cu -- the C ABI (include/tabi_gpu.h): argument checks, host <-> device
 // staging, and the order of the steps main.f90 performs.
 #include <algorithm>
+#include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <vector>
 
@@ -223,8 +226,11 @@ int tabi_form_matrix(tabi_h h, int nspt, const double* sptpos, const double* spt
     set_device(H);
     cudaStream_t s = H.stream;
     alloc_surface(H, nface);
-    DBuf<double> dpos, dnrm, dcp, dq;
-    DBuf<int> dfv;
+    DBuf<double>& dpos = H.st_pos;
+    DBuf<double>& dnrm = H.st_nrm;
+    DBuf<double>& dcp = H.st_cp;
+    DBuf<double>& dq = H.st_q;
+    DBuf<int>& dfv = H.st_fv;
     h2d(dpos, sptpos, 3 * (size_t)nspt, s);
     h2d(dnrm, sptnrm, 3 * (size_t)nspt, s);
     h2d(dfv, nvert, 3 * (size_t)nface, s);
@@ -233,11 +239,12 @@ int tabi_form_matrix(tabi_h h, int nspt, const double* sptpos, const double* spt
       h2d(dq, atmchr, (size_t)nchr, s);
     }
     pack_atoms_dev(H, nchr, dcp.p, dq.p, s);
-    DBuf<double> db;
+    DBuf<double>& db = H.st_b;
     db.alloc(2 * (size_t)nface);
     launch_form_matrix(H, nspt, dpos.p, dnrm.p, nface, dfv.p, nchr, H.d_atoms.p, db.p, s);
     if (tr_xyz || tr_q) {
-      DBuf<double> axyz, aq;
+      DBuf<double>& axyz = H.st_axyz;
+      DBuf<double>& aq = H.st_aq;
       axyz.alloc(3 * (size_t)nface);
       aq.alloc(3 * (size_t)nface);
       { TABI_K(K_FORM, s); aos_from_soa_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(
@@ -270,7 +277,9 @@ int tabi_set_surface(tabi_h h, int nface, const double* tr_xyz, const double* tr
     set_device(H);
     cudaStream_t s = H.stream;
     alloc_surface(H, nface);
-    DBuf<double> a, b, c;
+    DBuf<double>& a = H.st_axyz;
+    DBuf<double>& b = H.st_aq;
+    DBuf<double>& c = H.st_b;
     h2d(a, tr_xyz, 3 * (size_t)nface, s);
     h2d(b, tr_q, 3 * (size_t)nface, s);
     h2d(c, tr_area, (size_t)nface, s);
@@ -290,7 +299,9 @@ int tabi_rhs(tabi_h h, int nchr, const double* chrpos, const double* atmchr, dou
     TABI_REQUIRE(nchr > 0 && chrpos && atmchr && bvct, TABI_ERR_ARG, "bad atom arrays");
     set_device(H);
     cudaStream_t s = H.stream;
-    DBuf<double> dcp, dq, db;
+    DBuf<double>& dcp = H.st_cp;
+    DBuf<double>& dq = H.st_q;
+    DBuf<double>& db = H.st_b;
     h2d(dcp, chrpos, 3 * (size_t)nchr, s);
     h2d(dq, atmchr, (size_t)nchr, s);
     pack_atoms_dev(H, nchr, dcp.p, dq.p, s);
@@ -427,7 +438,9 @@ int tabi_energy(tabi_h h, int nchr, const double* chrpos, const double* atmchr, 
                  "bad energy arguments");
     set_device(H);
     cudaStream_t s = H.stream;
-    DBuf<double> dcp, dq, dx;
+    DBuf<double>& dcp = H.st_cp;
+    DBuf<double>& dq = H.st_q;
+    DBuf<double>& dx = H.st_x;
     h2d(dcp, chrpos, 3 * (size_t)nchr, s);
     h2d(dq, atmchr, (size_t)nchr, s);
     h2d(dx, x, 2 * (size_t)H.n, s);
@@ -454,17 +467,36 @@ int tabi_run_dev(tabi_h h, int nspt, const double* sptpos_dev, const double* spt
       cudaStream_t k;
       ~Restore() { H.stream = k; }
     } restore{H, keep};
+    // TABI_TRACE=1 prints host wall time per phase (synchronising between them)
+    static const bool trace = getenv("TABI_TRACE") && getenv("TABI_TRACE")[0] == '1';
+    auto t_last = std::chrono::steady_clock::now();
+    auto mark = [&](const char* what) {
+      if (!trace) return;
+      cudaStreamSynchronize(s);
+      auto t = std::chrono::steady_clock::now();
+      fprintf(stderr, "[tabi] %-12s %9.3f ms\n", what,
+              std::chrono::duration<double, std::milli>(t - t_last).count());
+      t_last = t;
+    };
     alloc_surface(H, nface);
     pack_atoms_dev(H, nchr, chrpos_dev, atmchr_dev, s);
-    DBuf<double> b0, b;
+    DBuf<double>& b0 = H.rn_b0;
+    DBuf<double>& b = H.rn_b;
     b0.alloc(2 * (size_t)nface);
     b.alloc(2 * (size_t)nface);
     launch_form_matrix(H, nspt, sptpos_dev, sptnrm_dev, nface, nvert_dev, nchr, H.d_atoms.p,
                        b0.p, s);
     H.has_surface = true;
-    do_build(H, s);
+    mark("form_matrix");
+    build_tree(H, s);
+    mark("tree");
+    build_lists(H, s);
+    H.has_tree = true;
+    mark("lists");
+    build_precond(H, s);
+    mark("precond");
     { TABI_K(K_FORM, s); permute_b_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(H.d_perm.p, nface, b0.p, b.p); }
-    DBuf<double> xl;
+    DBuf<double>& xl = H.rn_x;
     double* x = x_dev;
     if (!x) {
       xl.alloc(2 * (size_t)nface);
@@ -474,7 +506,9 @@ int tabi_run_dev(tabi_h h, int nspt, const double* sptpos_dev, const double* spt
     int iter = 0, ierr = 0;
     double err = 0.0, se = 0.0, ce = 0.0;
     gmres_dev(H, b.p, x, &iter, &err, &ierr, nullptr, nullptr, s);
+    mark("gmres");
     energy_dev(H, nchr, nullptr, nullptr, x, &se, &ce, s);
+    mark("energy");
     if (stats) {
       stats[0] = iter;
       stats[1] = err;

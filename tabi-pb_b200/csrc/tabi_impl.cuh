@@ -83,6 +83,21 @@ struct WorkItem {
 };
 
 struct Tree {
+  // Clears the host-side description; device buffers are kept and reused
+  // (they only ever grow), so rebuilding a tree allocates nothing once the
+  // sizes have been seen.
+  void clear() {
+    n = nnodes = nleaf = depth = 0;
+    ibeg.clear(); num.clear(); child0.clear(); nchild.clear(); level.clear();
+    mid.clear(); rad.clear(); leaves.clear();
+    n_near_pairs = n_far = n_slots = 0;
+    far_work.clear(); near_work.clear();
+    nmslot = 0;
+    mslot_node.clear(); mslot_chunk0.clear(); mslot_nchunk.clear();
+    blk_off.clear();
+    n_solve_big = n_solve_small = 0;
+    max_leaf = 0;
+  }
   int n = 0;          // faces
   int nnodes = 0;
   int nleaf = 0;
@@ -114,6 +129,8 @@ struct Tree {
   DBuf<int> d_piv;               // 2n per leaf, offsets 2*ibeg
   DBuf<int64_t> d_blk_off;
   DBuf<int2> d_leaf_rng;         // (ibeg, n) per leaf
+  DBuf<int> d_solve_list;        // leaves of the apply launches (big ones first)
+  int n_solve_big = 0, n_solve_small = 0;
   int max_leaf = 0;
 };
 
@@ -232,6 +249,19 @@ struct Handle {
   DBuf<int4> d_chunks;
   DBuf<int> d_cnt;
   DBuf<int> d_err;
+  // persistent workspaces of the build steps (grow-only)
+  DBuf<unsigned long long> tb_bb;
+  DBuf<double> tb_mid, tb_rad, tb_tmp;
+  DBuf<int> tb_split, tb_num;
+  DBuf<int> ls_tgt, ls_far, ls_near;
+  DBuf<int64_t> ls_bsum, ls_foff, ls_noff;
+  DBuf<int2> pc_tiles;
+  DBuf<int> pc_info, pc_list;
+  DBuf<int3> pc_items;
+  // staging of the host-array entry points and of tabi_run_dev
+  DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;
+  DBuf<int> st_fv;
+  DBuf<double> rn_b0, rn_b, rn_x;
 };
 
 // ---- kernels / launchers (defined in the .cu files) ----

@@ -377,7 +377,7 @@ void build_tree(Handle& H, cudaStream_t s) {
   Tree& T = H.tree;
   const int n = H.n;
   const int L = H.prm.maxparnode;
-  T = Tree();
+  T.clear();
   T.n = n;
   H.d_tx.alloc(n);
   H.d_ty.alloc(n);
@@ -388,10 +388,12 @@ void build_tree(Handle& H, cudaStream_t s) {
   H.d_err.alloc(1);
   { TABI_K(K_TREE, s); iota_kernel<<<ceil_div(n, 256), 256, 0, s>>>(H.d_perm.p, n); }
   // node table, grown per level
-  int cap = 1024;
-  DBuf<unsigned long long> bb;
-  DBuf<double> mid, rad;
-  DBuf<int> split, numd;
+  DBuf<unsigned long long>& bb = H.tb_bb;
+  DBuf<double>& mid = H.tb_mid;
+  DBuf<double>& rad = H.tb_rad;
+  DBuf<int>& split = H.tb_split;
+  DBuf<int>& numd = H.tb_num;
+  int cap = (int)std::min({bb.n / 6, mid.n / 3, rad.n, split.n, numd.n});
   auto ensure = [&](int need) {
     if (need <= cap && bb.p) return;
     int nc = std::max(need, 2 * cap);
@@ -582,7 +584,7 @@ void build_tree(Handle& H, cudaStream_t s) {
   H.d_tx.alloc(n);
   H.d_ty.alloc(n);
   H.d_tz.alloc(n);
-  DBuf<double> tarea;
+  DBuf<double>& tarea = H.tb_tmp;
   tarea.alloc(n);
   { TABI_K(K_TREE, s); gather4_kernel<<<ceil_div(n, 256), 256, 0, s>>>(H.d_perm.p, n, H.d_nx.p, H.d_ny.p, H.d_nz.p,
                                                   H.d_area.p, H.d_tx.p, H.d_ty.p, H.d_tz.p,
@@ -601,7 +603,9 @@ void build_lists(Handle& H, cudaStream_t s) {
   Tree& T = H.tree;
   const int n = H.n;
   const int nn = T.nnodes;
-  DBuf<int> tgt_cnt, far_cnt, near_cnt;
+  DBuf<int>& tgt_cnt = H.ls_tgt;
+  DBuf<int>& far_cnt = H.ls_far;
+  DBuf<int>& near_cnt = H.ls_near;
   tgt_cnt.alloc(n);
   far_cnt.alloc(nn);
   near_cnt.alloc(nn);
@@ -617,7 +621,7 @@ void build_lists(Handle& H, cudaStream_t s) {
   // per-target slot offsets (device scan)
   T.d_slot_off.alloc((size_t)n + 1);
   int nb = ceil_div(n, kScanB);
-  DBuf<int64_t> bsum;
+  DBuf<int64_t>& bsum = H.ls_bsum;
   bsum.alloc((size_t)nb + 1);
   { TABI_K(K_LISTS, s); scan_block_kernel<<<nb, kScanB, 0, s>>>(tgt_cnt.p, n, T.d_slot_off.p, bsum.p); }
   { TABI_K(K_LISTS, s); scan_top_kernel<<<1, 32, 0, s>>>(bsum.p, nb); }
@@ -644,7 +648,8 @@ void build_lists(Handle& H, cudaStream_t s) {
   T.n_near_pairs = pairs - n;  // every target meets its own leaf once
   TABI_REQUIRE(T.n_slots == tf + tn, TABI_ERR_CUDA, "interaction count mismatch");
   TABI_REQUIRE(T.n_slots < (1LL << 31), TABI_ERR_LIMIT, "more than 2^31 interactions");
-  DBuf<int64_t> d_foff, d_noff;
+  DBuf<int64_t>& d_foff = H.ls_foff;
+  DBuf<int64_t>& d_noff = H.ls_noff;
   d_foff.alloc(nn);
   d_noff.alloc(nn);
   TABI_CUDA(cudaMemcpyAsync(d_foff.p, foff.data(), sizeof(int64_t) * nn,
