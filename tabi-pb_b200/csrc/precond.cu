@@ -245,7 +245,7 @@ __global__ void __launch_bounds__(kLuThreads) lu_kernel(const int2* __restrict__
 //                     updates -- written back with its pivots;
 //   lu_update_kernel  one CTA per 128-column strip: the panel's row swaps,
 //                     then for strips right of the panel U12 = L11^{-1} A12 and
-//                     A22 -= L21 U12 (64 x 128 tiles, 4 x 8 per thread); strips
+//                     A22 -= L21 U12 (64 x 64 tiles, 4 x 4 per thread); strips
 //                     left of the panel only take the swaps (LAPACK applies
 //                     every pivot to the L columns too).
 // The trailing updates of all blocks run concurrently across the GPU.
@@ -342,7 +342,7 @@ __global__ void __launch_bounds__(kPT) lu_panel_kernel(const int* __restrict__ i
 }
 
 // item = (leaf, c0, c1): columns [c0, c1) of the leaf block
-__global__ void __launch_bounds__(kUT) lu_update_kernel(const int3* __restrict__ items, int k0,
+__global__ void __launch_bounds__(kUT, 2) lu_update_kernel(const int3* __restrict__ items, int k0,
                                                         const int2* __restrict__ leaf_rng,
                                                         const int64_t* __restrict__ blk_off,
                                                         double* __restrict__ lu,
@@ -352,6 +352,7 @@ __global__ void __launch_bounds__(kUT) lu_update_kernel(const int3* __restrict__
   __shared__ double sL[kUR][kBP + 1];
   __shared__ int s_rows[2 * kBP], s_src[2 * kBP];
   __shared__ int s_nr;
+  __shared__ double sV[2 * kBP][kUC / 2];
   const int3 it = items[blockIdx.x];
   const int leaf = it.x, c0 = it.y, c1 = it.z;
   const int2 lr = leaf_rng[leaf];
@@ -386,15 +387,20 @@ __global__ void __launch_bounds__(kUT) lu_update_kernel(const int3* __restrict__
   }
   __syncthreads();
   const int nr = s_nr;
-  if (tid < ncol) {
-    double* cc = A + (size_t)(c0 + tid) * m;
-    double v[2 * kBP];
-#pragma unroll
-    for (int q = 0; q < 2 * kBP; ++q)
-      if (q < nr) v[q] = cc[s_src[q]];
-#pragma unroll
-    for (int q = 0; q < 2 * kBP; ++q)
-      if (q < nr) cc[s_rows[q]] = v[q];
+  // apply the swaps: gather the involved rows of every strip column into
+  // shared memory, then scatter them to their destinations
+  for (int cs = 0; cs < ncol; cs += kUC / 2) {
+    const int nc = min(kUC / 2, ncol - cs);
+    for (int q = tid; q < nr * nc; q += kUT) {
+      int row = q / nc, c = q - row * nc;
+      sV[row][c] = A[(size_t)(c0 + cs + c) * m + s_src[row]];
+    }
+    __syncthreads();
+    for (int q = tid; q < nr * nc; q += kUT) {
+      int row = q / nc, c = q - row * nc;
+      A[(size_t)(c0 + cs + c) * m + s_rows[row]] = sV[row][c];
+    }
+    __syncthreads();
   }
   if (c1 <= k0) return;  // strip left of the panel: swaps only
   for (int q = tid; q < nb * nb; q += kUT) {
@@ -425,7 +431,8 @@ __global__ void __launch_bounds__(kUT) lu_update_kernel(const int3* __restrict__
 #pragma unroll
     for (int r = 0; r < kBP; ++r) sU[r][tid] = 0.0;
   }
-  // A22 -= L21 U12
+  // A22 -= L21 U12: 64-row tiles; each thread owns 4 rows x 4 columns of a
+  // 64 x 64 sub-tile, with the C values loaded before the products are formed
   const int tr = tid & 15, tc = tid >> 4;
   for (int r0 = k0 + nb; r0 < m; r0 += kUR) {
     __syncthreads();
@@ -435,125 +442,204 @@ __global__ void __launch_bounds__(kUT) lu_update_kernel(const int3* __restrict__
       sL[rr][k] = (gr < m && k < nb) ? A[(size_t)(k0 + k) * m + gr] : 0.0;
     }
     __syncthreads();
-    double acc[4][8];
+#pragma unroll 1
+    for (int ch = 0; ch < kUC; ch += 64) {
+      double cv[4][4], acc[4][4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int b = 0; b < 4; ++b) {
+        int c = ch + tc + 16 * b;
+        const double* cc = A + (size_t)(c0 + c) * m;
 #pragma unroll
-      for (int b = 0; b < 8; ++b) acc[a][b] = 0.0;
+        for (int a = 0; a < 4; ++a) {
+          int gr = r0 + tr + 16 * a;
+          cv[a][b] = (c < ncol && gr < m) ? cc[gr] : 0.0;
+          acc[a][b] = 0.0;
+        }
+      }
+#pragma unroll 4
+      for (int k = 0; k < kBP; ++k) {
+        double lv[4], uv[4];
 #pragma unroll
-    for (int k = 0; k < kBP; ++k) {
-      double lv[4], uv[8];
+        for (int a = 0; a < 4; ++a) lv[a] = sL[tr + 16 * a][k];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) lv[a] = sL[tr + 16 * a][k];
+        for (int b = 0; b < 4; ++b) uv[b] = sU[k][ch + tc + 16 * b];
 #pragma unroll
-      for (int b = 0; b < 8; ++b) uv[b] = sU[k][tc + 16 * b];
+        for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int a = 0; a < 4; ++a)
+          for (int b = 0; b < 4; ++b) acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
+      }
 #pragma unroll
-        for (int b = 0; b < 8; ++b) acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
-    }
+      for (int b = 0; b < 4; ++b) {
+        int c = ch + tc + 16 * b;
+        if (c >= ncol) continue;
+        double* cc = A + (size_t)(c0 + c) * m;
 #pragma unroll
-    for (int b = 0; b < 8; ++b) {
-      int c = tc + 16 * b;
-      if (c >= ncol) continue;
-      double* cc = A + (size_t)(c0 + c) * m;
-#pragma unroll
-      for (int a = 0; a < 4; ++a) {
-        int gr = r0 + tr + 16 * a;
-        if (gr < m) cc[gr] -= acc[a][b];
+        for (int a = 0; a < 4; ++a) {
+          int gr = r0 + tr + 16 * a;
+          if (gr < m) cc[gr] = cv[a][b] - acc[a][b];
+        }
       }
     }
   }
 }
 
-// Forward/back substitution with the factored block (DGETRS 'N'): 32-row
-// blocks; the diagonal 32 x 32 triangle is staged in shared memory and solved
-// by one warp, the rows below (above) are updated with a 32-wide GEMV by all
-// threads.  Large blocks run with 1024 threads so that each of the m/16
-// sequential block steps is short; leaf_list selects the leaves of a launch.
+// After the factorisation, per leaf: the row permutation of all its pivots
+// (DLASWP applied to the index vector, so an apply gathers in one parallel
+// step) and the inverses of the 32 x 32 diagonal blocks of L (unit lower) and
+// U (upper), so that each step of the blocked substitutions is a small GEMV
+// instead of a 32-step serial recurrence.
+constexpr int kDB = 32;
+
+__global__ void lu_perm_kernel(const int2* __restrict__ leaf_rng, const int* __restrict__ piv,
+                               int nleaf, int* __restrict__ perm) {
+  int leaf = blockIdx.x * blockDim.x + threadIdx.x;
+  if (leaf >= nleaf) return;
+  int2 lr = leaf_rng[leaf];
+  int m = 2 * lr.y;
+  const int* ip = piv + 2 * lr.x;
+  int* pm = perm + 2 * lr.x;
+  for (int i = 0; i < m; ++i) pm[i] = i;
+  for (int k = 0; k < m; ++k) {
+    int p = ip[k] - 1;
+    if (p != k) {
+      int t = pm[k];
+      pm[k] = pm[p];
+      pm[p] = t;
+    }
+  }
+}
+
+// one warp per (leaf, diagonal block): lane j computes column j of L^{-1} and
+// U^{-1} of the block (identity padding past the end of the matrix)
+__global__ void lu_diaginv_kernel(const int2* __restrict__ blocks,  // (leaf, k0)
+                                  const int2* __restrict__ leaf_rng,
+                                  const int64_t* __restrict__ blk_off,
+                                  const int64_t* __restrict__ dinv_off,
+                                  const double* __restrict__ lu, double* __restrict__ dinv) {
+  __shared__ double D[4][kDB][kDB + 1];
+  int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  int2 bk = blocks[blockIdx.x * 4 + w];
+  if (bk.x < 0) return;
+  int2 lr = leaf_rng[bk.x];
+  int m = 2 * lr.y, k0 = bk.y, nb = min(kDB, m - k0);
+  const double* A = lu + blk_off[bk.x];
+  for (int c = 0; c < kDB; ++c)
+    D[w][lane][c] = (c < nb && lane < nb) ? A[(size_t)(k0 + c) * m + k0 + lane]
+                                          : (c == lane ? 1.0 : 0.0);
+  __syncwarp();
+  double* Li = dinv + dinv_off[bk.x] + (size_t)(k0 / kDB) * 2 * kDB * kDB;
+  double* Ui = Li + kDB * kDB;
+  // L^{-1} e_j (unit lower)
+  double x[kDB];
+#pragma unroll
+  for (int i = 0; i < kDB; ++i) {
+    double v = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+    for (int q = 0; q < kDB; ++q)
+      if (q < i) v = fma(-D[w][i][q], x[q], v);
+    x[i] = v;
+  }
+#pragma unroll
+  for (int i = 0; i < kDB; ++i) Li[(size_t)lane * kDB + i] = x[i];  // column lane
+  // U^{-1} e_j (upper, non-unit)
+#pragma unroll
+  for (int i = kDB - 1; i >= 0; --i) {
+    double v = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+    for (int q = 0; q < kDB; ++q)
+      if (q > i) v = fma(-D[w][i][q], x[q], v);
+    x[i] = v / D[w][i][i];
+  }
+#pragma unroll
+  for (int i = 0; i < kDB; ++i) Ui[(size_t)lane * kDB + i] = x[i];
+}
+
+// Forward/back substitution with the factored block (DGETRS 'N') in 32-row
+// steps: gather through the pivot permutation, then per step the diagonal
+// block is applied as a 32 x 32 GEMV with its precomputed inverse (one warp)
+// and the rows below (above) are updated with a 32-wide GEMV by all threads.
+// Large blocks run with 512 threads; leaf_list selects the launch's leaves.
 template <int NT>
-__global__ void __launch_bounds__(NT) solve_kernel(
+__global__ void __launch_bounds__(NT, 1) solve_kernel(
     const int2* __restrict__ leaf_rng, const int64_t* __restrict__ blk_off,
-    const int* __restrict__ leaf_list, const double* __restrict__ lu,
-    const int* __restrict__ piv, int N, const double* __restrict__ r,
+    const int64_t* __restrict__ dinv_off, const int* __restrict__ leaf_list,
+    const double* __restrict__ lu, const double* __restrict__ dinv,
+    const int* __restrict__ perm, int N, const double* __restrict__ r,
     double* __restrict__ z) {
   extern __shared__ double xs[];
-  __shared__ double D[32][33];
   int leaf = leaf_list[blockIdx.x];
   int2 lr = leaf_rng[leaf];
-  int n = lr.y, m = 2 * n, ib = lr.x;
+  const int n = lr.y, m = 2 * n, ib = lr.x;
   const double* A = lu + blk_off[leaf];
-  const int* ip = piv + 2 * ib;
-  int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int i = tid; i < n; i += blockDim.x) {
-    xs[i] = r[ib + i];
-    xs[n + i] = r[N + ib + i];
+  const double* Di = dinv + dinv_off[leaf];
+  const int* pm = perm + 2 * ib;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int i = tid; i < m; i += NT) {
+    int src = pm[i];
+    xs[i] = (src < n) ? r[ib + src] : r[N + ib + src - n];
   }
   __syncthreads();
-  if (tid == 0)  // DLASWP, increasing k
-    for (int k = 0; k < m; ++k) {
-      int p = ip[k] - 1;
-      if (p != k) {
-        double t = xs[k];
-        xs[k] = xs[p];
-        xs[p] = t;
-      }
-    }
-  // L y = P r (unit lower)
-  for (int k0 = 0; k0 < m; k0 += 32) {
-    int nb = min(32, m - k0);
-    for (int q = tid; q < nb * nb; q += blockDim.x) {
-      int c = q / nb, rr = q - c * nb;
-      D[rr][c] = A[(size_t)(k0 + c) * m + k0 + rr];
-    }
-    __syncthreads();
+  // L y = P r
+  for (int k0 = 0; k0 < m; k0 += kDB) {
+    const int nb = min(kDB, m - k0);
     if (warp == 0) {
-      double v = (lane < nb) ? xs[k0 + lane] : 0.0;
-      for (int kk = 0; kk < nb; ++kk) {
-        double xk = __shfl_sync(0xffffffffu, v, kk);
-        if (lane > kk && lane < nb) v = fma(-D[lane][kk], xk, v);
-      }
+      const double* Li = Di + (size_t)(k0 / kDB) * 2 * kDB * kDB;
+      double v = 0.0;
+#pragma unroll
+      for (int q = 0; q < kDB; ++q)
+        if (q < nb) v = fma(Li[(size_t)q * kDB + lane], xs[k0 + q], v);
+      __syncwarp();
       if (lane < nb) xs[k0 + lane] = v;
     }
     __syncthreads();
-    for (int i = k0 + nb + tid; i < m; i += blockDim.x) {
-      double s = xs[i];
+    for (int i = k0 + nb + tid; i < m; i += NT) {
       const double* a = A + (size_t)k0 * m + i;
-#pragma unroll 8
-      for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], xs[k0 + q], s);
+      double s = xs[i];
+      if (nb == kDB) {
+        double t[kDB];
+#pragma unroll
+        for (int q = 0; q < kDB; ++q) t[q] = a[(size_t)q * m];
+#pragma unroll
+        for (int q = 0; q < kDB; ++q) s = fma(-t[q], xs[k0 + q], s);
+      } else {
+        for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], xs[k0 + q], s);
+      }
       xs[i] = s;
     }
     __syncthreads();
   }
   // U x = y
-  for (int kend = m; kend > 0; kend -= 32) {
-    int k0 = max(0, kend - 32);
-    int nb = kend - k0;
-    for (int q = tid; q < nb * nb; q += blockDim.x) {
-      int c = q / nb, rr = q - c * nb;
-      D[rr][c] = A[(size_t)(k0 + c) * m + k0 + rr];
-    }
-    __syncthreads();
+  const int nblk = (m + kDB - 1) / kDB;
+  for (int b = nblk - 1; b >= 0; --b) {
+    const int k0 = b * kDB;
+    const int nb = min(kDB, m - k0);
     if (warp == 0) {
-      double v = (lane < nb) ? xs[k0 + lane] : 0.0;
-      for (int kk = nb - 1; kk >= 0; --kk) {
-        if (lane == kk) v = v / D[kk][kk];
-        double xk = __shfl_sync(0xffffffffu, v, kk);
-        if (lane < kk) v = fma(-D[lane][kk], xk, v);
-      }
+      const double* Ui = Di + (size_t)b * 2 * kDB * kDB + kDB * kDB;
+      double v = 0.0;
+#pragma unroll
+      for (int q = 0; q < kDB; ++q)
+        if (q < nb) v = fma(Ui[(size_t)q * kDB + lane], xs[k0 + q], v);
+      __syncwarp();
       if (lane < nb) xs[k0 + lane] = v;
     }
     __syncthreads();
-    for (int i = tid; i < k0; i += blockDim.x) {
-      double s = xs[i];
+    for (int i = tid; i < k0; i += NT) {
       const double* a = A + (size_t)k0 * m + i;
-#pragma unroll 8
-      for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], xs[k0 + q], s);
+      double s = xs[i];
+      if (nb == kDB) {
+        double t[kDB];
+#pragma unroll
+        for (int q = 0; q < kDB; ++q) t[q] = a[(size_t)q * m];
+#pragma unroll
+        for (int q = 0; q < kDB; ++q) s = fma(-t[q], xs[k0 + q], s);
+      } else {
+        for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], xs[k0 + q], s);
+      }
       xs[i] = s;
     }
     __syncthreads();
   }
-  for (int i = tid; i < n; i += blockDim.x) {
+  for (int i = tid; i < n; i += NT) {
     z[ib + i] = xs[i];
     z[N + ib + i] = xs[n + i];
   }
@@ -663,7 +749,7 @@ void build_precond(Handle& H, cudaStream_t s) {
             d_info.p);
       }
       if (nu > 0) {
-        TABI_K(K_LU, s);
+        TABI_K(K_LU_UPDATE, s);
         lu_update_kernel<<<nu, kUT, 0, s>>>(H.pc_items.p + uoff[st], k0, T.d_leaf_rng.p,
                                             T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
       }
@@ -682,7 +768,32 @@ void build_precond(Handle& H, cudaStream_t s) {
       throw Error(TABI_ERR_SINGULAR, "leaf block " + std::to_string(l) +
                                          " is singular (DGETRF info " +
                                          std::to_string(info[l]) + ")");
-  // apply lists: blocks of order > 256 (largest first) get 1024 threads
+  // pivot permutations and inverse diagonal blocks for the applies
+  {
+    T.dinv_off.resize(nl);
+    int64_t doff = 0;
+    std::vector<int2> dblocks;
+    for (int l = 0; l < nl; ++l) {
+      T.dinv_off[l] = doff;
+      int m = 2 * rng[l].y;
+      int nblk = (m + kDB - 1) / kDB;
+      doff += (int64_t)nblk * 2 * kDB * kDB;
+      for (int b = 0; b < nblk; ++b) dblocks.push_back(make_int2(l, b * kDB));
+    }
+    while (dblocks.size() % 4) dblocks.push_back(make_int2(-1, 0));
+    T.d_dinv.alloc(std::max<int64_t>(doff, 1));
+    T.d_dinv_off.alloc(nl);
+    T.d_lu_perm.alloc(2 * (size_t)H.n);
+    H.pc_dblocks.alloc(std::max<size_t>(dblocks.size(), 1));
+    TABI_CUDA(cudaMemcpyAsync(T.d_dinv_off.p, T.dinv_off.data(), sizeof(int64_t) * nl,
+                              cudaMemcpyHostToDevice, s));
+    TABI_CUDA(cudaMemcpyAsync(H.pc_dblocks.p, dblocks.data(), sizeof(int2) * dblocks.size(),
+                              cudaMemcpyHostToDevice, s));
+    { TABI_K(K_LU_POST, s); lu_perm_kernel<<<ceil_div(nl, 64), 64, 0, s>>>(T.d_leaf_rng.p, T.d_piv.p, nl, T.d_lu_perm.p); }
+    { TABI_K(K_LU_POST, s); lu_diaginv_kernel<<<(int)(dblocks.size() / 4), 128, 0, s>>>(
+        H.pc_dblocks.p, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_lu.p, T.d_dinv.p); }
+  }
+  // apply lists: blocks of order > 256 (largest first) get 512 threads
   {
     std::vector<int> big, small;
     for (int l = 0; l < nl; ++l) (2 * rng[l].y > 256 ? big : small).push_back(l);
@@ -713,20 +824,20 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
   if (smem > 48 * 1024) {
     TABI_CUDA(cudaFuncSetAttribute(solve_kernel<256>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TABI_CUDA(cudaFuncSetAttribute(solve_kernel<1024>,
+    TABI_CUDA(cudaFuncSetAttribute(solve_kernel<512>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
   if (T.n_solve_big > 0) {
     TABI_K(K_SOLVE, s);
-    solve_kernel<1024><<<T.n_solve_big, 1024, smem, s>>>(T.d_leaf_rng.p, T.d_blk_off.p,
-                                                         T.d_solve_list.p, T.d_lu.p, T.d_piv.p,
-                                                         n, r, z);
+    solve_kernel<512><<<T.n_solve_big, 512, smem, s>>>(
+        T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_solve_list.p, T.d_lu.p, T.d_dinv.p,
+        T.d_lu_perm.p, n, r, z);
   }
   if (T.n_solve_small > 0) {
     TABI_K(K_SOLVE, s);
-    solve_kernel<256><<<T.n_solve_small, 256, smem, s>>>(T.d_leaf_rng.p, T.d_blk_off.p,
-                                                         T.d_solve_list.p + T.n_solve_big,
-                                                         T.d_lu.p, T.d_piv.p, n, r, z);
+    solve_kernel<256><<<T.n_solve_small, 256, smem, s>>>(
+        T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_solve_list.p + T.n_solve_big,
+        T.d_lu.p, T.d_dinv.p, T.d_lu_perm.p, n, r, z);
   }
   TABI_CUDA(cudaGetLastError());
 }

@@ -595,9 +595,10 @@ int tabi_profile_read(tabi_h h, int kclass, double* ms, int64_t* launches) {
 int tabi_profile_nclasses(void) { return K_NCLASS; }
 
 const char* tabi_profile_class_name(int kclass) {
-  static const char* names[K_NCLASS] = {"form_matrix", "tree", "lists",   "moments",
-                                        "far",         "near", "reduce",  "assemble",
-                                        "lu",          "solve", "vector", "energy"};
+  static const char* names[K_NCLASS] = {"form_matrix", "tree",   "lists",     "moments",
+                                        "far",         "near",   "reduce",    "assemble",
+                                        "lu_panel",    "solve",  "vector",    "energy",
+                                        "lu_update",   "lu_post"};
   return (kclass >= 0 && kclass < K_NCLASS) ? names[kclass] : "all";
 }
 

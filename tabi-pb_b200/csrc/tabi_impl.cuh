@@ -95,6 +95,7 @@ struct Tree {
     nmslot = 0;
     mslot_node.clear(); mslot_chunk0.clear(); mslot_nchunk.clear();
     blk_off.clear();
+    dinv_off.clear();
     n_solve_big = n_solve_small = 0;
     max_leaf = 0;
   }
@@ -130,6 +131,10 @@ struct Tree {
   DBuf<int64_t> d_blk_off;
   DBuf<int2> d_leaf_rng;         // (ibeg, n) per leaf
   DBuf<int> d_solve_list;        // leaves of the apply launches (big ones first)
+  std::vector<int64_t> dinv_off;  // per leaf offset of its inverse diagonal blocks
+  DBuf<int64_t> d_dinv_off;
+  DBuf<double> d_dinv;           // per 32-row block: L^{-1}, U^{-1} (32 x 32 each)
+  DBuf<int> d_lu_perm;           // per leaf row permutation of all pivots
   int n_solve_big = 0, n_solve_small = 0;
   int max_leaf = 0;
 };
@@ -137,7 +142,7 @@ struct Tree {
 // Kernel classes for the launch counters / event timers (tabi_profile_*).
 enum KClass {
   K_FORM = 0, K_TREE, K_LISTS, K_MOMENTS, K_FAR, K_NEAR, K_REDUCE, K_ASSEMBLE, K_LU,
-  K_SOLVE, K_VEC, K_ENERGY, K_NCLASS
+  K_SOLVE, K_VEC, K_ENERGY, K_LU_UPDATE, K_LU_POST, K_NCLASS
 };
 
 struct Handle;
@@ -258,6 +263,7 @@ struct Handle {
   DBuf<int2> pc_tiles;
   DBuf<int> pc_info, pc_list;
   DBuf<int3> pc_items;
+  DBuf<int2> pc_dblocks;
   // staging of the host-array entry points and of tabi_run_dev
   DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;
   DBuf<int> st_fv;
