@@ -145,6 +145,27 @@ int tabi_energy_dev(tabi_h h, int nchr, const double* chrpos_dev,
                     const double* atmchr_dev, const double* x_dev,
                     double* soleng, double* couleng, void* stream);
 
+/* Solvation and Coulomb energy as tabi_energy, for callers that cannot
+ * allocate device memory (device memory owned and budgeted by another
+ * allocator, or a pipeline that cannot absorb the device-wide
+ * synchronisation of cudaFree).  No counterpart in the reference.
+ * Allocates nothing: needs no handle; its scratch is a file-scope static
+ * device array of 2^20 doubles (8 MiB) that every GPU which loads the library
+ * holds until exit.  All pointers are device pointers on the current device:
+ * the surface in the reference's layout (tr_xyz, tr_q 3 x nface, tr_area),
+ * x (2 nface, same face order), atoms (chrpos 3 x nchr, atmchr); out receives
+ * [soleng, couleng] (kcal/mol).  nchr <= 524288, else TABI_ERR_LIMIT.  The
+ * first call on a device looks up the scratch address (cudaGetSymbolAddress)
+ * and should come before any stream capture.  Every call writes the scratch
+ * it reads, nothing needs clearing; calls that overlap on the GPU (on
+ * different streams) share the scratch and race. */
+int tabi_energy_noalloc(int nface, const double* tr_xyz_dev,
+                        const double* tr_q_dev, const double* tr_area_dev,
+                        const double* x_dev, int nchr,
+                        const double* chrpos_dev, const double* atmchr_dev,
+                        double kappa, double eps0, double eps1,
+                        double* out_dev, void* stream);
+
 /* Whole path on device-resident inputs (form_matrix, tree, preconditioner,
  * GMRES, energy) -- one call per molecule.  Inputs as tabi_form_matrix but
  * device pointers; x_dev (2 nface, tree order on return) may be NULL.

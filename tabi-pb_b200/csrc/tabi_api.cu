@@ -13,6 +13,9 @@
 namespace tabi {
 void pack_atoms_dev(Handle& H, int nchr, const double* chrpos_dev, const double* atmchr_dev,
                     cudaStream_t s);
+void energy_noalloc(int nface, const double* tr_xyz, const double* tr_q, const double* tr_area,
+                    const double* x, int nchr, const double* chrpos, const double* atmchr,
+                    double kappa, double eps0, double eps1, double* out, cudaStream_t s);
 }
 
 using namespace tabi;
@@ -446,6 +449,16 @@ int tabi_energy(tabi_h h, int nchr, const double* chrpos, const double* atmchr, 
     h2d(dx, x, 2 * (size_t)H.n, s);
     pack_atoms_dev(H, nchr, dcp.p, dq.p, s);
     energy_dev(H, nchr, nullptr, nullptr, dx.p, soleng, couleng, s);
+  });
+}
+
+int tabi_energy_noalloc(int nface, const double* tr_xyz_dev, const double* tr_q_dev,
+                        const double* tr_area_dev, const double* x_dev, int nchr,
+                        const double* chrpos_dev, const double* atmchr_dev, double kappa,
+                        double eps0, double eps1, double* out_dev, void* stream) {
+  return guarded(nullptr, [&] {
+    energy_noalloc(nface, tr_xyz_dev, tr_q_dev, tr_area_dev, x_dev, nchr, chrpos_dev, atmchr_dev,
+                   kappa, eps0, eps1, out_dev, (cudaStream_t)stream);
   });
 }
 

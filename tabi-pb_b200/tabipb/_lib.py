@@ -29,7 +29,7 @@ SYMBOLS = [
     "tabi_matvec_dev", "tabi_msolve", "tabi_msolve_dev", "tabi_solve", "tabi_solve_dev",
     "tabi_energy", "tabi_energy_dev", "tabi_run_dev", "tabi_counts", "tabi_tree_nodes",
     "tabi_probe_fp64_peak", "tabi_profile_enable", "tabi_profile_read", "tabi_profile_nclasses",
-    "tabi_profile_class_name",
+    "tabi_profile_class_name", "tabi_energy_noalloc",
 ]
 
 
@@ -92,6 +92,8 @@ def load(path: str = LIB_PATH):
     L.tabi_profile_nclasses.argtypes = []
     L.tabi_profile_class_name.argtypes = [C.c_int]
     L.tabi_profile_class_name.restype = C.c_char_p
+    L.tabi_energy_noalloc.argtypes = [C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.c_double,
+                                      C.c_double, C.c_double, _vp, _vp]
     for s in SYMBOLS:
         if s not in ("tabi_default_params", "tabi_kappa", "tabi_last_error",
                      "tabi_profile_class_name"):
