@@ -71,7 +71,26 @@ def build(force: bool = False, jobs: int = 6, verbose_ptxas: bool = False) -> st
     if force or not os.path.exists(LIB) or _mtime(LIB) < max(_mtime(o) for o in objs):
         cmd = [nvcc(), *ARCH, "-shared", "-o", LIB, *objs, "-lcudart"]
         subprocess.run(cmd, check=True)
+    build_driver(force)
     return LIB
+
+
+def build_driver(force: bool = False) -> str:
+    """tabipb (host driver mirroring main.f90) and tabi_msms next to the library."""
+    src = os.path.join(PKG, "host", "tabipb_main.cpp")
+    exe = os.path.join(OUT, "tabipb")
+    hdr = os.path.join(PKG, "..", "include", "tabi_gpu.h")
+    cxx = "/usr/bin/g++" if os.path.exists("/usr/bin/g++") else "g++"
+    if force or _mtime(exe) < max(_mtime(src), _mtime(hdr), _mtime(LIB)):
+        subprocess.run([cxx, "-O2", "-std=c++17", "-o", exe, src, "-L" + OUT, "-ltabi_gpu",
+                        "-Wl,-rpath,$ORIGIN"], check=True)
+    sg = os.path.join(PKG, "surfgen")
+    msms = os.path.join(OUT, "tabi_msms")
+    srcs = [os.path.join(sg, f) for f in ("tabi_msms.c", "surfgen.c", "surfgen.h")]
+    if force or _mtime(msms) < max(map(_mtime, srcs)):
+        cc = "/usr/bin/gcc" if os.path.exists("/usr/bin/gcc") else "gcc"
+        subprocess.run([cc, "-O2", "-o", msms, srcs[0], srcs[1], "-lm"], check=True)
+    return exe
 
 
 if __name__ == "__main__":

@@ -11,6 +11,8 @@
 //                                    linear combination of the Krylov vectors,
 //                                    fused with its norm (ISDGMR :2532-2650),
 //   DPIGMR final update (:1836-1848) one linear combination.
+#include <cooperative_groups.h>
+
 #include <cmath>
 #include <vector>
 
@@ -71,6 +73,80 @@ __global__ void sub_kernel(int n, const double* __restrict__ b, double* __restri
 }
 
 constexpr int kVecBlocks = 592;
+constexpr int kOrthThreads = 256;
+
+// Sum of part[0..np) in a fixed order, identical in every block.
+__device__ __forceinline__ double block_sum_parts(const double* part, int np, double* sm) {
+  double v = 0.0;
+  for (int i = threadIdx.x; i < np; i += blockDim.x) v += part[i];
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sm[k];
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ void block_partial(double acc, double* part, double* sm) {
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) t += sm[k];
+    part[blockIdx.x] = t;
+  }
+  __syncthreads();
+}
+
+// DORTH's modified Gram-Schmidt (dgmres_dep.f:1376-1395) in one cooperative
+// launch: out[maxlp1] = |vn|^2 before, out[i-1] = h_i = V_i . vn followed by
+// vn -= h_i V_i for i = i0..ll in order, out[maxlp1+1] = |vn|^2 after.  Each
+// thread owns the same elements in every pass, so an axpy and the next dot
+// need no barrier; the partial sums are double-buffered and every block adds
+// them in the same order, so all blocks see the same h_i.
+__global__ void __launch_bounds__(kOrthThreads) dorth_kernel(const double* __restrict__ V,
+                                                            int64_t ld, int n, int i0, int ll,
+                                                            int maxlp1, double* __restrict__ vn,
+                                                            double* __restrict__ part,
+                                                            double* __restrict__ out) {
+  namespace cg = cooperative_groups;
+  cg::grid_group grid = cg::this_grid();
+  __shared__ double sm[kOrthThreads / 32];
+  const int np = gridDim.x;
+  const int stride = gridDim.x * blockDim.x;
+  const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+  int buf = 0;
+  double acc = 0.0;
+  for (int k = t0; k < n; k += stride) acc = fma(vn[k], vn[k], acc);
+  block_partial(acc, part + buf * np, sm);
+  grid.sync();
+  {
+    double s = block_sum_parts(part + buf * np, np, sm);
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[maxlp1] = s;
+  }
+  for (int i = i0; i <= ll; ++i) {
+    const double* vi = V + (int64_t)(i - 1) * ld;
+    buf ^= 1;
+    acc = 0.0;
+    for (int k = t0; k < n; k += stride) acc = fma(vi[k], vn[k], acc);
+    block_partial(acc, part + buf * np, sm);
+    grid.sync();
+    const double h = block_sum_parts(part + buf * np, np, sm);
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[i - 1] = h;
+    for (int k = t0; k < n; k += stride) vn[k] = fma(-h, vi[k], vn[k]);
+  }
+  buf ^= 1;
+  acc = 0.0;
+  for (int k = t0; k < n; k += stride) acc = fma(vn[k], vn[k], acc);
+  block_partial(acc, part + buf * np, sm);
+  grid.sync();
+  {
+    double s = block_sum_parts(part + buf * np, np, sm);
+    if (blockIdx.x == 0 && threadIdx.x == 0) out[maxlp1 + 1] = s;
+  }
+}
 
 void givens(double t1, double t2, double& c, double& s) {
   if (t2 == 0.0) {
@@ -110,6 +186,18 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
   H.d_r.alloc(n);
   H.d_coef.alloc(4 * (size_t)maxlp1 + kRedBlocks + 8);
   H.d_red.alloc(kRedBlocks + 8);
+  // cooperative DORTH: every block must be resident
+  int orth_blocks = 0;
+  {
+    int per_sm = 0, nsm = 0, dev = 0;
+    TABI_CUDA(cudaGetDevice(&dev));
+    TABI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    TABI_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, dorth_kernel, kOrthThreads, 0));
+    orth_blocks = std::max(1, std::min(2, per_sm)) * nsm;
+    orth_blocks = std::min(orth_blocks, std::max(1, ceil_div(n, kOrthThreads)));
+  }
+  H.d_orth.alloc(2 * (size_t)orth_blocks + 8);
+  double* d_orth_part = H.d_orth.p;
   double* V = H.d_v.p;
   double* wk = H.d_wk.p;
   double* dl = H.d_dl.p;
@@ -167,17 +255,21 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
         double* vn = Vc(ll + 1);
         matvec_dev(H, Vc(ll), wk, s, false);  // |V(:,ll)| = 1: never the zero shortcut
         msolve_dev(H, wk, vn, s);
-        // ---- DORTH
-        { TABI_K(K_VEC, s); reduce_partial_kernel<2><<<kRedBlocks, kRedThreads, 0, s>>>(vn, nullptr, n, d_part); }
-        { TABI_K(K_VEC, s); reduce_final_kernel<<<1, 256, 0, s>>>(d_part, kRedBlocks, d_h + maxlp1); }  // vnrm^2
+        // ---- DORTH: one cooperative launch for the whole sweep
         int i0 = std::max(1, ll - kmp + 1);
-        for (int i = i0; i <= ll; ++i) {
-          { TABI_K(K_VEC, s); reduce_partial_kernel<1><<<kRedBlocks, kRedThreads, 0, s>>>(Vc(i), vn, n, d_part); }
-          { TABI_K(K_VEC, s); reduce_final_kernel<<<1, 256, 0, s>>>(d_part, kRedBlocks, d_h + (i - 1)); }
-          { TABI_K(K_VEC, s); axpy_dcoef_kernel<<<vb, vt, 0, s>>>(n, d_h + (i - 1), -1.0, Vc(i), vn); }
+        {
+          TABI_K(K_VEC, s);
+          const double* Vp = V;
+          int64_t ldv = n;
+          int nn = n, ii0 = i0, lll = ll, mlp1 = maxlp1;
+          double* vnp = vn;
+          double* pp = d_orth_part;
+          double* op = d_h;
+          void* args[] = {(void*)&Vp, (void*)&ldv, (void*)&nn, (void*)&ii0, (void*)&lll,
+                          (void*)&mlp1, (void*)&vnp, (void*)&pp, (void*)&op};
+          TABI_CUDA(cudaLaunchCooperativeKernel((const void*)dorth_kernel, dim3(orth_blocks),
+                                                dim3(kOrthThreads), args, 0, s));
         }
-        { TABI_K(K_VEC, s); reduce_partial_kernel<2><<<kRedBlocks, kRedThreads, 0, s>>>(vn, nullptr, n, d_part); }
-        { TABI_K(K_VEC, s); reduce_final_kernel<<<1, 256, 0, s>>>(d_part, kRedBlocks, d_h + maxlp1 + 1); }
         TABI_CUDA(cudaMemcpyAsync(H.h_pinned, d_h, sizeof(double) * (maxlp1 + 2),
                                   cudaMemcpyDeviceToHost, s));
         TABI_CUDA(cudaStreamSynchronize(s));

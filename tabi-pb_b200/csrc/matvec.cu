@@ -292,6 +292,22 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
     }
   }
   Tree& T = H.tree;
+  TABI_PHASE(K_PHASE_MATVEC, s);
+  // the near field runs on the handle's side stream, concurrently with the
+  // moments + far field on s; both write disjoint result slots
+  const bool fork = !T.near_work.empty() && H.side != nullptr;
+  cudaStream_t sn = fork ? H.side : s;
+  if (fork) {
+    TABI_CUDA(cudaEventRecord(H.ev_fork, s));
+    TABI_CUDA(cudaStreamWaitEvent(sn, H.ev_fork, 0));
+  }
+  if (!T.near_work.empty()) {
+    TABI_K(K_NEAR, sn);
+    near_kernel<<<(int)T.near_work.size(), kNearThreads, 0, sn>>>(
+        T.d_near_work.p, T.d_near_ent.p, T.d_ibeg.p, T.d_num.p, H.d_x.p, H.d_y.p, H.d_z.p,
+        H.d_nx.p, H.d_ny.p, H.d_nz.p, H.d_area.p, x, n, H.prm.kappa, H.prm.eps1 / H.prm.eps0,
+        H.d_res.p);
+  }
   switch (H.prm.order) {
     case 1: launch_order<1>(H, x, y, s); break;
     case 2: launch_order<2>(H, x, y, s); break;
@@ -303,11 +319,10 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
     case 8: launch_order<8>(H, x, y, s); break;
     default: throw Error(TABI_ERR_ARG, "order must be 1..8");
   }
-  if (!T.near_work.empty())
-    { TABI_K(K_NEAR, s); near_kernel<<<(int)T.near_work.size(), kNearThreads, 0, s>>>(
-        T.d_near_work.p, T.d_near_ent.p, T.d_ibeg.p, T.d_num.p, H.d_x.p, H.d_y.p, H.d_z.p,
-        H.d_nx.p, H.d_ny.p, H.d_nz.p, H.d_area.p, x, n, H.prm.kappa,
-        H.prm.eps1 / H.prm.eps0, H.d_res.p); }
+  if (fork) {
+    TABI_CUDA(cudaEventRecord(H.ev_join, sn));
+    TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
+  }
   double eps = H.prm.eps1 / H.prm.eps0;
   { TABI_K(K_REDUCE, s); reduce_kernel<<<ceil_div(n, 256), 256, 0, s>>>(T.d_slot_off.p, H.d_res.p, x, n,
                                                  0.5 * (1.0 + eps), 0.5 * (1.0 + 1.0 / eps), y); }

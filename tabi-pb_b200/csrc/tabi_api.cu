@@ -191,6 +191,9 @@ int tabi_create(tabi_h* h, const tabi_params* p) {
     nh->H.prm = *p;
     TABI_CUDA(cudaGetDevice(&nh->H.device));
     TABI_CUDA(cudaStreamCreateWithFlags(&nh->H.stream, cudaStreamNonBlocking));
+    TABI_CUDA(cudaStreamCreateWithFlags(&nh->H.side, cudaStreamNonBlocking));
+    TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_fork, cudaEventDisableTiming));
+    TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_join, cudaEventDisableTiming));
     TABI_CUDA(cudaMallocHost(&nh->H.h_pinned, sizeof(double) * 256));
   });
   if (rc != TABI_OK) {
@@ -206,9 +209,14 @@ int tabi_destroy(tabi_h h) {
   cudaSetDevice(h->H.device);
   if (h->H.stream) cudaStreamSynchronize(h->H.stream);
   if (h->H.h_pinned) cudaFreeHost(h->H.h_pinned);
-  cudaStream_t s = h->H.stream;
+  if (h->H.side) cudaStreamSynchronize(h->H.side);
+  cudaStream_t s = h->H.stream, s2 = h->H.side;
+  cudaEvent_t e1 = h->H.ev_fork, e2 = h->H.ev_join;
   delete h;
   if (s) cudaStreamDestroy(s);
+  if (s2) cudaStreamDestroy(s2);
+  if (e1) cudaEventDestroy(e1);
+  if (e2) cudaEventDestroy(e2);
   return TABI_OK;
 }
 
@@ -596,7 +604,7 @@ int tabi_profile_read(tabi_h h, int kclass, double* ms, int64_t* launches) {
     double t = 0.0;
     int64_t l = 0;
     for (int k = 0; k < K_NCLASS; ++k)
-      if (kclass == -1 || kclass == k) {
+      if ((kclass == -1 && k != K_PHASE_MATVEC) || kclass == k) {
         t += H.prof.ms[k];
         l += H.prof.launches[k];
       }
@@ -611,7 +619,7 @@ const char* tabi_profile_class_name(int kclass) {
   static const char* names[K_NCLASS] = {"form_matrix", "tree",   "lists",     "moments",
                                         "far",         "near",   "reduce",    "assemble",
                                         "lu_panel",    "solve",  "vector",    "energy",
-                                        "lu_update",   "lu_post"};
+                                        "lu_update",   "lu_post",   "matvec"};
   return (kclass >= 0 && kclass < K_NCLASS) ? names[kclass] : "all";
 }
 

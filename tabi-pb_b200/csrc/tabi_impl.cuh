@@ -142,7 +142,9 @@ struct Tree {
 // Kernel classes for the launch counters / event timers (tabi_profile_*).
 enum KClass {
   K_FORM = 0, K_TREE, K_LISTS, K_MOMENTS, K_FAR, K_NEAR, K_REDUCE, K_ASSEMBLE, K_LU,
-  K_SOLVE, K_VEC, K_ENERGY, K_LU_UPDATE, K_LU_POST, K_NCLASS
+  K_SOLVE, K_VEC, K_ENERGY, K_LU_UPDATE, K_LU_POST,
+  K_PHASE_MATVEC,  // whole treecode matvec (a phase: timed, not a launch)
+  K_NCLASS
 };
 
 struct Handle;
@@ -202,7 +204,7 @@ struct KScope {
   cudaStream_t s;
   cudaEvent_t a = nullptr;
   KScope(Prof& p, int k, cudaStream_t st) : P(p), kind(k), s(st) {
-    P.launches[kind]++;
+    P.launches[kind]++;  // for a phase class: the number of times it ran
     if (P.on) {
       a = P.get();
       cudaEventRecord(a, s);
@@ -217,12 +219,15 @@ struct KScope {
   }
 };
 #define TABI_K(kind, s) ::tabi::KScope _kscope_(H.prof, (kind), (s))
+#define TABI_PHASE(kind, s) ::tabi::KScope _pscope_(H.prof, (kind), (s))
 
 struct Handle {
   tabi_params prm{};
   Prof prof;
   std::string err;
   cudaStream_t stream = nullptr;
+  cudaStream_t side = nullptr;           // second stream of the matvec (near field)
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int device = 0;
   int n = 0;  // faces
   bool has_surface = false, has_tree = false, has_precond = false;
@@ -241,7 +246,7 @@ struct Handle {
   double* h_pinned = nullptr;  // small pinned host scratch (64 doubles)
   // GMRES workspace
   DBuf<double> d_v, d_wk, d_dl, d_gz, d_r, d_b, d_xio, d_tmp;
-  DBuf<double> d_coef;
+  DBuf<double> d_coef, d_orth;
   // energy scratch
   DBuf<double> d_ptl;
   DBuf<double> d_atoms;

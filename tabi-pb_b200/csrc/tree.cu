@@ -665,7 +665,7 @@ void build_lists(Handle& H, cudaStream_t s) {
       T.d_rad.p, H.prm.theta, nullptr, nullptr, nullptr, T.d_slot_off.p, d_foff.p, d_noff.p,
       far_cnt.p, near_cnt.p, T.d_far_ent.p, T.d_near_ent.p, H.d_err.p); }
   // work items and moment slots
-  const int kFarChunk = 64, kNearChunk = 128, kMomChunk = 2048;
+  const int kFarChunk = 64, kNearChunk = 128, kMomChunk = 256;
   T.far_work.clear();
   T.near_work.clear();
   T.mslot_node.clear();
