@@ -231,24 +231,33 @@ __global__ void reduce_kernel(const int64_t* __restrict__ slot_off,
 }
 
 template <int P>
-void launch_order(Handle& H, const double* x, double* y, cudaStream_t s) {
+void launch_moments(Handle& H, const double* x, cudaStream_t s) {
   Tree& T = H.tree;
-  const int n = H.n;
   constexpr int NT = tabi_nterms(P);
-  if (T.nmslot > 0) {
-    int nch = 0;
-    for (int k = 0; k < T.nmslot; ++k) nch += T.mslot_nchunk[k];
-    int threads = ((4 * NT + 31) / 32) * 32;
-    { TABI_K(K_MOMENTS, s); mom_partial_kernel<P><<<nch, threads, 0, s>>>(T.d_mchunks.p, T.d_mslot_node.p, T.d_mid.p,
-                                                  H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p,
-                                                  H.d_ny.p, H.d_nz.p, H.d_area.p, x, n,
-                                                  H.d_mraw.p); }
-    { TABI_K(K_MOMENTS, s); mom_final_kernel<P><<<T.nmslot, 256, 0, s>>>(T.d_mslot_chunks.p, H.d_mraw.p, H.d_mw.p); }
+  if (T.nmslot == 0) return;
+  int nch = 0;
+  for (int k = 0; k < T.nmslot; ++k) nch += T.mslot_nchunk[k];
+  int threads = ((4 * NT + 31) / 32) * 32;
+  {
+    TABI_K(K_MOMENTS, s);
+    mom_partial_kernel<P><<<nch, threads, 0, s>>>(T.d_mchunks.p, T.d_mslot_node.p, T.d_mid.p,
+                                                  H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p, H.d_ny.p,
+                                                  H.d_nz.p, H.d_area.p, x, H.n, H.d_mraw.p);
   }
-  if (!T.far_work.empty())
-    { TABI_K(K_FAR, s); far_kernel<P><<<(int)T.far_work.size(), 64, 0, s>>>(
-        T.d_far_work.p, T.d_far_ent.p, H.d_mw.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p,
-        H.d_nx.p, H.d_ny.p, H.d_nz.p, H.prm.kappa, H.prm.eps1 / H.prm.eps0, H.d_res.p); }
+  {
+    TABI_K(K_MOMENTS, s);
+    mom_final_kernel<P><<<T.nmslot, 256, 0, s>>>(T.d_mslot_chunks.p, H.d_mraw.p, H.d_mw.p);
+  }
+}
+
+template <int P>
+void launch_far(Handle& H, cudaStream_t s) {
+  Tree& T = H.tree;
+  if (T.far_work.empty()) return;
+  TABI_K(K_FAR, s);
+  far_kernel<P><<<(int)T.far_work.size(), 64, 0, s>>>(
+      T.d_far_work.p, T.d_far_ent.p, H.d_mw.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p,
+      H.d_ny.p, H.d_nz.p, H.prm.kappa, H.prm.eps1 / H.prm.eps0, H.d_res.p);
 }
 
 }  // namespace
@@ -301,6 +310,19 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
     TABI_CUDA(cudaEventRecord(H.ev_fork, s));
     TABI_CUDA(cudaStreamWaitEvent(sn, H.ev_fork, 0));
   }
+  // moments first (small, needed by the far field), then the near field on
+  // the side stream and the far field on s
+  switch (H.prm.order) {
+    case 1: launch_moments<1>(H, x, s); break;
+    case 2: launch_moments<2>(H, x, s); break;
+    case 3: launch_moments<3>(H, x, s); break;
+    case 4: launch_moments<4>(H, x, s); break;
+    case 5: launch_moments<5>(H, x, s); break;
+    case 6: launch_moments<6>(H, x, s); break;
+    case 7: launch_moments<7>(H, x, s); break;
+    case 8: launch_moments<8>(H, x, s); break;
+    default: throw Error(TABI_ERR_ARG, "order must be 1..8");
+  }
   if (!T.near_work.empty()) {
     TABI_K(K_NEAR, sn);
     near_kernel<<<(int)T.near_work.size(), kNearThreads, 0, sn>>>(
@@ -309,15 +331,15 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
         H.d_res.p);
   }
   switch (H.prm.order) {
-    case 1: launch_order<1>(H, x, y, s); break;
-    case 2: launch_order<2>(H, x, y, s); break;
-    case 3: launch_order<3>(H, x, y, s); break;
-    case 4: launch_order<4>(H, x, y, s); break;
-    case 5: launch_order<5>(H, x, y, s); break;
-    case 6: launch_order<6>(H, x, y, s); break;
-    case 7: launch_order<7>(H, x, y, s); break;
-    case 8: launch_order<8>(H, x, y, s); break;
-    default: throw Error(TABI_ERR_ARG, "order must be 1..8");
+    case 1: launch_far<1>(H, s); break;
+    case 2: launch_far<2>(H, s); break;
+    case 3: launch_far<3>(H, s); break;
+    case 4: launch_far<4>(H, s); break;
+    case 5: launch_far<5>(H, s); break;
+    case 6: launch_far<6>(H, s); break;
+    case 7: launch_far<7>(H, s); break;
+    case 8: launch_far<8>(H, s); break;
+    default: break;
   }
   if (fork) {
     TABI_CUDA(cudaEventRecord(H.ev_join, sn));

@@ -237,52 +237,43 @@ __global__ void __launch_bounds__(kLuThreads) lu_kernel(const int2* __restrict__
 
 
 // Batched, level-synchronous right-looking LU with partial pivoting for all
-// leaf blocks of order m <= kPanelMaxM at once.  Panel step s (k0 = 16 s) is
-// two launches over every block that still has columns left:
-//   lu_panel_kernel   one CTA per block: the 16-column panel (rows k0..m-1)
-//                     in shared memory -- pivot search (largest |a|, first
-//                     index on ties, as IDAMAX), row swap, scaling, rank-1
-//                     updates -- written back with its pivots;
-//   lu_update_kernel  one CTA per 128-column strip: the panel's row swaps,
-//                     then for strips right of the panel U12 = L11^{-1} A12 and
-//                     A22 -= L21 U12 (64 x 64 tiles, 4 x 4 per thread); strips
-//                     left of the panel only take the swaps (LAPACK applies
-//                     every pivot to the L columns too).
+// leaf blocks of order m <= kPanelMaxM at once.  Panel step s (k0 = 32 s) is
+// three launches over every block that still has columns left:
+//   lu_panel_kernel  one CTA per block: the 32-column panel (rows k0..m-1),
+//                    as two 16-column halves in shared memory -- pivot search
+//                    (largest |a|, first index on ties, as IDAMAX), row swap,
+//                    scaling, rank-1 updates; the second half first takes the
+//                    first half's swaps, TRSM and GEMM update (DGETRF2's
+//                    recursion, one level);
+//   lu_strip_kernel  one CTA per 128-column strip: the panel's row swaps
+//                    (gathered through shared memory), and for strips right of
+//                    the panel U12 = L11^{-1} A12; strips left of the panel
+//                    only take swaps (LAPACK applies every pivot to the L
+//                    columns too; the panel kernel applies its second half's
+//                    swaps to its first half);
+//   lu_gemm_kernel   one CTA per 64 x 64 tile of every trailing matrix:
+//                    A22 -= L21 U12 with k = 32, C loaded before the products.
 // The trailing updates of all blocks run concurrently across the GPU.
-constexpr int kBP = 16;            // panel width
-constexpr int kPanelMaxM = 1536;   // panel of 1536 x 16 doubles = 192 KB of smem
+constexpr int kBP = 32;            // panel width
+constexpr int kSP = 16;            // panel half held in shared memory
+constexpr int kPanelMaxM = 1536;   // half panel of 1536 x 16 doubles = 192 KB
 constexpr int kPT = 256;           // panel kernel threads
-constexpr int kUT = 256;           // update kernel threads
+constexpr int kUT = 256;           // strip / gemm kernel threads
 constexpr int kUC = 128;           // strip width
-constexpr int kUR = 64;            // row tile of the update
+constexpr int kGT = 64;            // gemm tile
 
-__global__ void __launch_bounds__(kPT) lu_panel_kernel(const int* __restrict__ items, int k0,
-                                                       const int2* __restrict__ leaf_rng,
-                                                       const int64_t* __restrict__ blk_off,
-                                                       double* __restrict__ lu,
-                                                       int* __restrict__ piv,
-                                                       int* __restrict__ info) {
-  extern __shared__ double P[];
-  __shared__ double s_v[kPT / 32];
-  __shared__ int s_i[kPT / 32];
-  __shared__ int s_p;
-  const int leaf = items[blockIdx.x];
-  const int2 lr = leaf_rng[leaf];
-  const int m = 2 * lr.y;
-  const int nb = min(kBP, m - k0), mr = m - k0;
-  double* A = lu + blk_off[leaf];
-  int* ip = piv + 2 * lr.x;
+// Factor columns [c0l, c0l + nb) of the panel held in P (local column c of
+// the half is P + c * mr, local row r = global row k0 + r) starting at local
+// row r0; records 1-based global pivots.
+__device__ void panel_factor(double* P, int mr, int r0, int nb, int k0, int* ip, int* info,
+                             int leaf, double* s_v, int* s_i, int* s_p) {
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  for (int q = tid; q < nb * mr; q += kPT) {
-    int c = q / mr, r = q - c * mr;
-    P[q] = A[(size_t)(k0 + c) * m + k0 + r];
-  }
-  __syncthreads();
   for (int j = 0; j < nb; ++j) {
+    const int lr0 = r0 + j;  // local row of the diagonal
     double* col = P + (size_t)j * mr;
     double bv = -1.0;
     int bi = mr;
-    for (int i = j + tid; i < mr; i += kPT) argmax_merge(bv, bi, fabs(col[i]), i);
+    for (int i = lr0 + tid; i < mr; i += kPT) argmax_merge(bv, bi, fabs(col[i]), i);
     for (int o = 16; o > 0; o >>= 1) {
       double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
       int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
@@ -301,79 +292,202 @@ __global__ void __launch_bounds__(kPT) lu_panel_kernel(const int* __restrict__ i
         int i2 = __shfl_xor_sync(0xffffffffu, i, o);
         argmax_merge(v, i, v2, i2);
       }
-      if (lane == 0) s_p = i;
+      if (lane == 0) *s_p = i;
     }
     __syncthreads();
-    int p = s_p;
+    const int p = *s_p;
     const double pv = col[p];
     if (pv == 0.0) {  // DGETRF2: INFO set, no swap, no scaling
       if (tid == 0) {
-        atomicCAS(&info[leaf], 0, k0 + j + 1);
-        ip[k0 + j] = k0 + j + 1;
+        atomicCAS(&info[leaf], 0, k0 + lr0 + 1);
+        ip[k0 + lr0] = k0 + lr0 + 1;
       }
       __syncthreads();
       continue;
     }
-    if (tid == 0) ip[k0 + j] = k0 + p + 1;  // 1-based, like LAPACK
-    if (p != j && tid < nb) {
+    if (tid == 0) ip[k0 + lr0] = k0 + p + 1;  // 1-based, like LAPACK
+    if (p != lr0 && tid < nb) {
       double* cc = P + (size_t)tid * mr;
-      double t = cc[j];
-      cc[j] = cc[p];
+      double t = cc[lr0];
+      cc[lr0] = cc[p];
       cc[p] = t;
     }
     __syncthreads();
-    const double pk = col[j];
+    const double pk = col[lr0];
     const bool recip = fabs(pk) >= 2.2250738585072014e-308;
     const double rcp = 1.0 / pk;
-    for (int i = j + 1 + tid; i < mr; i += kPT) {
+    for (int i = lr0 + 1 + tid; i < mr; i += kPT) {
       double l = recip ? col[i] * rcp : col[i] / pk;
       col[i] = l;
       for (int c = j + 1; c < nb; ++c) {
         double* cc = P + (size_t)c * mr;
-        cc[i] = fma(-l, cc[j], cc[i]);
+        cc[i] = fma(-l, cc[lr0], cc[i]);
       }
     }
     __syncthreads();
   }
-  for (int q = tid; q < nb * mr; q += kPT) {
+}
+
+__global__ void __launch_bounds__(kPT) lu_panel_kernel(const int* __restrict__ items, int k0,
+                                                       const int2* __restrict__ leaf_rng,
+                                                       const int64_t* __restrict__ blk_off,
+                                                       double* __restrict__ lu,
+                                                       int* __restrict__ piv,
+                                                       int* __restrict__ info) {
+  extern __shared__ double P[];
+  __shared__ double s_v[kPT / 32];
+  __shared__ int s_i[kPT / 32];
+  __shared__ int s_p;
+  __shared__ double sL11[kSP][kSP + 1];
+  __shared__ int s_rows[2 * kSP], s_src[2 * kSP];
+  const int leaf = items[blockIdx.x];
+  const int2 lr = leaf_rng[leaf];
+  const int m = 2 * lr.y;
+  const int nb = min(kBP, m - k0), mr = m - k0;
+  const int nb1 = min(kSP, nb), nb2 = nb - nb1;
+  double* A = lu + blk_off[leaf];
+  int* ip = piv + 2 * lr.x;
+  const int tid = threadIdx.x;
+  // ---- first half
+  for (int q = tid; q < nb1 * mr; q += kPT) {
+    int c = q / mr, r = q - c * mr;
+    P[q] = A[(size_t)(k0 + c) * m + k0 + r];
+  }
+  __syncthreads();
+  panel_factor(P, mr, 0, nb1, k0, ip, info, leaf, s_v, s_i, &s_p);
+  for (int q = tid; q < nb1 * mr; q += kPT) {
     int c = q / mr, r = q - c * mr;
     A[(size_t)(k0 + c) * m + k0 + r] = P[q];
   }
-}
-
-// item = (leaf, c0, c1): columns [c0, c1) of the leaf block
-__global__ void __launch_bounds__(kUT, 2) lu_update_kernel(const int3* __restrict__ items, int k0,
-                                                        const int2* __restrict__ leaf_rng,
-                                                        const int64_t* __restrict__ blk_off,
-                                                        double* __restrict__ lu,
-                                                        const int* __restrict__ piv) {
-  __shared__ double sL11[kBP][kBP + 1];
-  __shared__ double sU[kBP][kUC];
-  __shared__ double sL[kUR][kBP + 1];
-  __shared__ int s_rows[2 * kBP], s_src[2 * kBP];
-  __shared__ int s_nr;
-  __shared__ double sV[2 * kBP][kUC / 2];
-  const int3 it = items[blockIdx.x];
-  const int leaf = it.x, c0 = it.y, c1 = it.z;
-  const int2 lr = leaf_rng[leaf];
-  const int m = 2 * lr.y;
-  const int nb = min(kBP, m - k0);
-  double* A = lu + blk_off[leaf];
-  const int* ip = piv + 2 * lr.x;
-  const int tid = threadIdx.x;
-  const int ncol = c1 - c0;
-  // rows touched by the panel's swaps and, for each, the row its value comes from
+  if (nb2 == 0) return;
+  for (int q = tid; q < nb1 * nb1; q += kPT) {
+    int c = q / nb1, r = q - c * nb1;
+    sL11[r][c] = P[(size_t)c * mr + r];
+  }
+  __syncthreads();
+  // ---- second half: load, first half's swaps, TRSM, GEMM update, factor
+  const int c2 = k0 + kSP;
+  for (int q = tid; q < nb2 * mr; q += kPT) {
+    int c = q / mr, r = q - c * mr;
+    P[q] = A[(size_t)(c2 + c) * m + k0 + r];
+  }
+  __syncthreads();
+  if (tid < nb2) {
+    double* cc = P + (size_t)tid * mr;
+    for (int j = 0; j < nb1; ++j) {
+      int p = ip[k0 + j] - 1 - k0;
+      if (p != j) {
+        double t = cc[j];
+        cc[j] = cc[p];
+        cc[p] = t;
+      }
+    }
+    double x[kSP];
+#pragma unroll
+    for (int r = 0; r < kSP; ++r) x[r] = (r < nb1) ? cc[r] : 0.0;
+#pragma unroll
+    for (int r = 1; r < kSP; ++r) {
+      double acc = x[r];
+#pragma unroll
+      for (int q = 0; q < kSP; ++q)
+        if (q < r) acc = fma(-sL11[r][q], x[q], acc);
+      x[r] = acc;
+    }
+#pragma unroll
+    for (int r = 0; r < kSP; ++r)
+      if (r < nb1) cc[r] = x[r];
+  }
+  __syncthreads();
+  // rows kSP.. of the second half -= L21 (first half, global) * U (rows 0..15 of P)
+  for (int i = kSP + tid; i < mr; i += kPT) {
+    double l[kSP];
+#pragma unroll
+    for (int q = 0; q < kSP; ++q) l[q] = A[(size_t)(k0 + q) * m + k0 + i];
+    for (int c = 0; c < nb2; ++c) {
+      double* cc = P + (size_t)c * mr;
+      double acc = cc[i];
+#pragma unroll
+      for (int q = 0; q < kSP; ++q) acc = fma(-l[q], cc[q], acc);
+      cc[i] = acc;
+    }
+  }
+  __syncthreads();
+  panel_factor(P, mr, kSP, nb2, k0, ip, info, leaf, s_v, s_i, &s_p);
+  for (int q = tid; q < nb2 * mr; q += kPT) {
+    int c = q / mr, r = q - c * mr;
+    A[(size_t)(c2 + c) * m + k0 + r] = P[q];
+  }
+  // the second half's swaps on the first half's columns (gathered through
+  // shared memory: rows touched and, for each, the row its value comes from)
+  __syncthreads();
   if (tid == 0) {
     int nr = 0;
-    for (int j = 0; j < nb; ++j) s_rows[nr++] = k0 + j;
-    for (int j = 0; j < nb; ++j) {
+    for (int j = kSP; j < nb; ++j) s_rows[nr++] = k0 + j;
+    for (int j = kSP; j < nb; ++j) {
       int p = ip[k0 + j] - 1;
       bool have = false;
       for (int q = 0; q < nr; ++q) have |= (s_rows[q] == p);
       if (!have) s_rows[nr++] = p;
     }
     for (int q = 0; q < nr; ++q) s_src[q] = s_rows[q];
-    for (int j = 0; j < nb; ++j) {  // content[] of the rows after each swap, in order
+    for (int j = kSP; j < nb; ++j) {
+      int p = ip[k0 + j] - 1, a = -1, b = -1;
+      for (int q = 0; q < nr; ++q) {
+        if (s_rows[q] == k0 + j) a = q;
+        if (s_rows[q] == p) b = q;
+      }
+      int t = s_src[a];
+      s_src[a] = s_src[b];
+      s_src[b] = t;
+    }
+    s_p = nr;
+  }
+  __syncthreads();
+  const int nr = s_p;
+  for (int q = tid; q < nr * nb1; q += kPT) {
+    int row = q / nb1, c = q - row * nb1;
+    P[q] = A[(size_t)(k0 + c) * m + s_src[row]];
+  }
+  __syncthreads();
+  for (int q = tid; q < nr * nb1; q += kPT) {
+    int row = q / nb1, c = q - row * nb1;
+    A[(size_t)(k0 + c) * m + s_rows[row]] = P[q];
+  }
+}
+
+// item = (leaf, c0, c1, mode): columns [c0, c1) of the leaf block.
+// mode 0: left of the panel, the panel's swaps; 1: right of the panel, the
+// panel's swaps then U12 = L11^{-1} A12.
+__global__ void __launch_bounds__(kUT) lu_strip_kernel(const int4* __restrict__ items, int k0,
+                                                       const int2* __restrict__ leaf_rng,
+                                                       const int64_t* __restrict__ blk_off,
+                                                       double* __restrict__ lu,
+                                                       const int* __restrict__ piv) {
+  __shared__ double sL11[kBP][kBP + 1];
+  __shared__ double sV[2 * kBP][kUC / 2];
+  __shared__ int s_rows[2 * kBP], s_src[2 * kBP];
+  __shared__ int s_nr;
+  const int4 it = items[blockIdx.x];
+  const int leaf = it.x, c0 = it.y, c1 = it.z, mode = it.w;
+  const int2 lr = leaf_rng[leaf];
+  const int m = 2 * lr.y;
+  const int nb = min(kBP, m - k0);
+  const int pj0 = 0;
+  double* A = lu + blk_off[leaf];
+  const int* ip = piv + 2 * lr.x;
+  const int tid = threadIdx.x;
+  const int ncol = c1 - c0;
+  if (tid == 0) {
+    int nr = 0;
+    for (int j = pj0; j < nb; ++j) s_rows[nr++] = k0 + j;
+    for (int j = pj0; j < nb; ++j) {
+      int p = ip[k0 + j] - 1;
+      bool have = false;
+      for (int q = 0; q < nr; ++q) have |= (s_rows[q] == p);
+      if (!have) s_rows[nr++] = p;
+    }
+    for (int q = 0; q < nr; ++q) s_src[q] = s_rows[q];
+    for (int j = pj0; j < nb; ++j) {  // content of the rows after each swap, in order
       int p = ip[k0 + j] - 1, a = -1, b = -1;
       for (int q = 0; q < nr; ++q) {
         if (s_rows[q] == k0 + j) a = q;
@@ -387,8 +501,6 @@ __global__ void __launch_bounds__(kUT, 2) lu_update_kernel(const int3* __restric
   }
   __syncthreads();
   const int nr = s_nr;
-  // apply the swaps: gather the involved rows of every strip column into
-  // shared memory, then scatter them to their destinations
   for (int cs = 0; cs < ncol; cs += kUC / 2) {
     const int nc = min(kUC / 2, ncol - cs);
     for (int q = tid; q < nr * nc; q += kUT) {
@@ -402,14 +514,13 @@ __global__ void __launch_bounds__(kUT, 2) lu_update_kernel(const int3* __restric
     }
     __syncthreads();
   }
-  if (c1 <= k0) return;  // strip left of the panel: swaps only
+  if (mode != 1) return;
   for (int q = tid; q < nb * nb; q += kUT) {
     int c = q / nb, r = q - c * nb;
     sL11[r][c] = A[(size_t)(k0 + c) * m + k0 + r];
   }
   __syncthreads();
-  // U12 = L11^{-1} A12 (unit lower), one column per thread
-  if (tid < ncol) {
+  if (tid < ncol) {  // U12 = L11^{-1} A12 (unit lower), one column per thread
     double* cc = A + (size_t)(c0 + tid) * m;
     double x[kBP];
 #pragma unroll
@@ -423,62 +534,71 @@ __global__ void __launch_bounds__(kUT, 2) lu_update_kernel(const int3* __restric
       x[r] = acc;
     }
 #pragma unroll
-    for (int r = 0; r < kBP; ++r) {
+    for (int r = 0; r < kBP; ++r)
       if (r < nb) cc[k0 + r] = x[r];
-      sU[r][tid] = (r < nb) ? x[r] : 0.0;
-    }
-  } else if (tid < kUC) {
-#pragma unroll
-    for (int r = 0; r < kBP; ++r) sU[r][tid] = 0.0;
   }
-  // A22 -= L21 U12: 64-row tiles; each thread owns 4 rows x 4 columns of a
-  // 64 x 64 sub-tile, with the C values loaded before the products are formed
-  const int tr = tid & 15, tc = tid >> 4;
-  for (int r0 = k0 + nb; r0 < m; r0 += kUR) {
-    __syncthreads();
-    for (int q = tid; q < kUR * kBP; q += kUT) {
-      int k = q / kUR, rr = q - k * kUR;
-      int gr = r0 + rr;
-      sL[rr][k] = (gr < m && k < nb) ? A[(size_t)(k0 + k) * m + gr] : 0.0;
+}
+
+// item = (leaf, r0, c0): C[r0:r0+64, c0:c0+64] -= L21[r0:, k0:k0+nb] U12[k0:k0+nb, c0:]
+__global__ void __launch_bounds__(kUT) lu_gemm_kernel(const int4* __restrict__ items, int k0,
+                                                      const int2* __restrict__ leaf_rng,
+                                                      const int64_t* __restrict__ blk_off,
+                                                      double* __restrict__ lu) {
+  __shared__ double sL[kBP][kGT + 1];
+  __shared__ double sU[kBP][kGT + 1];
+  const int4 it = items[blockIdx.x];
+  const int leaf = it.x, r0 = it.y, c0 = it.z;
+  const int m = 2 * leaf_rng[leaf].y;
+  const int nb = min(kBP, m - k0);
+  double* A = lu + blk_off[leaf];
+  const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
+  // C values first (independent of the tiles)
+  double cv[4][4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = c0 + tc + 16 * b;
+    const double* cc = A + (size_t)c * m;
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + tr + 16 * a;
+      cv[a][b] = (c < m && r < m) ? cc[r] : 0.0;
     }
-    __syncthreads();
-#pragma unroll 1
-    for (int ch = 0; ch < kUC; ch += 64) {
-      double cv[4][4], acc[4][4];
+  }
+  for (int q = tid; q < kBP * kGT; q += kUT) {
+    int k = q / kGT, rr = q - k * kGT;
+    int r = r0 + rr;
+    sL[k][rr] = (k < nb && r < m) ? A[(size_t)(k0 + k) * m + r] : 0.0;
+    int k2 = q % kBP, cc2 = q / kBP;
+    int c = c0 + cc2;
+    sU[k2][cc2] = (k2 < nb && c < m) ? A[(size_t)c * m + k0 + k2] : 0.0;
+  }
+  __syncthreads();
+  double acc[4][4];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        int c = ch + tc + 16 * b;
-        const double* cc = A + (size_t)(c0 + c) * m;
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          int gr = r0 + tr + 16 * a;
-          cv[a][b] = (c < ncol && gr < m) ? cc[gr] : 0.0;
-          acc[a][b] = 0.0;
-        }
-      }
-#pragma unroll 4
-      for (int k = 0; k < kBP; ++k) {
-        double lv[4], uv[4];
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+#pragma unroll 8
+  for (int k = 0; k < kBP; ++k) {
+    double lv[4], uv[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) lv[a] = sL[tr + 16 * a][k];
+    for (int a = 0; a < 4; ++a) lv[a] = sL[k][tr + 16 * a];
 #pragma unroll
-        for (int b = 0; b < 4; ++b) uv[b] = sU[k][ch + tc + 16 * b];
+    for (int b = 0; b < 4; ++b) uv[b] = sU[k][tc + 16 * b];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < 4; ++a)
 #pragma unroll
-          for (int b = 0; b < 4; ++b) acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
-      }
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
+  }
 #pragma unroll
-      for (int b = 0; b < 4; ++b) {
-        int c = ch + tc + 16 * b;
-        if (c >= ncol) continue;
-        double* cc = A + (size_t)(c0 + c) * m;
+  for (int b = 0; b < 4; ++b) {
+    const int c = c0 + tc + 16 * b;
+    if (c >= m) continue;
+    double* cc = A + (size_t)c * m;
 #pragma unroll
-        for (int a = 0; a < 4; ++a) {
-          int gr = r0 + tr + 16 * a;
-          if (gr < m) cc[gr] = cv[a][b] - acc[a][b];
-        }
-      }
+    for (int a = 0; a < 4; ++a) {
+      const int r = r0 + tr + 16 * a;
+      if (r < m) cc[r] = cv[a][b] - acc[a][b];
     }
   }
 }
@@ -706,52 +826,67 @@ void build_precond(Handle& H, cudaStream_t s) {
     for (int l = 0; l < nl; ++l) order[l] = l;
     std::sort(order.begin(), order.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
     std::vector<int> pitems;
-    std::vector<int3> uitems;
-    std::vector<int> poff(nsteps + 1), uoff(nsteps + 1);
+    std::vector<int4> sitems, gitems;
+    std::vector<int> poff(nsteps + 1), soff(nsteps + 1), goff(nsteps + 1);
     for (int st = 0; st < nsteps; ++st) {
       const int k0 = st * kBP;
       poff[st] = (int)pitems.size();
-      uoff[st] = (int)uitems.size();
+      soff[st] = (int)sitems.size();
+      goff[st] = (int)gitems.size();
       for (int l : order) {
         const int m = 2 * rng[l].y;
         if (m > kPanelMaxM || m <= k0) continue;
         pitems.push_back(l);
         const int nb = std::min(kBP, m - k0);
-        for (int c0 = 0; c0 < k0; c0 += kUC) uitems.push_back(make_int3(l, c0, std::min(c0 + kUC, k0)));
+        for (int c0 = 0; c0 < k0; c0 += kUC)
+          sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, k0), 0));
         for (int c0 = k0 + nb; c0 < m; c0 += kUC)
-          uitems.push_back(make_int3(l, c0, std::min(c0 + kUC, m)));
+          sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, m), 1));
+        for (int r0 = k0 + nb; r0 < m; r0 += kGT)
+          for (int c0 = k0 + nb; c0 < m; c0 += kGT) gitems.push_back(make_int4(l, r0, c0, 0));
       }
     }
     poff[nsteps] = (int)pitems.size();
-    uoff[nsteps] = (int)uitems.size();
+    soff[nsteps] = (int)sitems.size();
+    goff[nsteps] = (int)gitems.size();
     H.pc_list.alloc(std::max<size_t>(pitems.size(), 1));
-    H.pc_items.alloc(std::max<size_t>(uitems.size(), 1));
+    H.pc_items.alloc(std::max<size_t>(sitems.size(), 1));
+    H.pc_gitems.alloc(std::max<size_t>(gitems.size(), 1));
     if (!pitems.empty())
       TABI_CUDA(cudaMemcpyAsync(H.pc_list.p, pitems.data(), sizeof(int) * pitems.size(),
                                 cudaMemcpyHostToDevice, s));
-    if (!uitems.empty())
-      TABI_CUDA(cudaMemcpyAsync(H.pc_items.p, uitems.data(), sizeof(int3) * uitems.size(),
+    if (!sitems.empty())
+      TABI_CUDA(cudaMemcpyAsync(H.pc_items.p, sitems.data(), sizeof(int4) * sitems.size(),
+                                cudaMemcpyHostToDevice, s));
+    if (!gitems.empty())
+      TABI_CUDA(cudaMemcpyAsync(H.pc_gitems.p, gitems.data(), sizeof(int4) * gitems.size(),
                                 cudaMemcpyHostToDevice, s));
     if (nsteps > 0) {
-      size_t smem = sizeof(double) * (size_t)mmax * kBP;
+      size_t smem = sizeof(double) * (size_t)mmax * kSP;
       TABI_CUDA(cudaFuncSetAttribute(lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)std::max<size_t>(smem, 48 * 1024)));
     }
     for (int st = 0; st < nsteps; ++st) {
       const int k0 = st * kBP;
-      const int np = poff[st + 1] - poff[st], nu = uoff[st + 1] - uoff[st];
-      // panel rows: the largest block still active at this step
-      const int mr = 2 * rng[pitems[poff[st]]].y - k0;
+      const int np = poff[st + 1] - poff[st], ns = soff[st + 1] - soff[st],
+                ng = goff[st + 1] - goff[st];
       if (np > 0) {
+        // shared memory for the largest block still active at this step
+        const int mr = 2 * rng[pitems[poff[st]]].y - k0;
         TABI_K(K_LU, s);
-        lu_panel_kernel<<<np, kPT, sizeof(double) * (size_t)mr * kBP, s>>>(
+        lu_panel_kernel<<<np, kPT, sizeof(double) * (size_t)mr * kSP, s>>>(
             H.pc_list.p + poff[st], k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
             d_info.p);
       }
-      if (nu > 0) {
+      if (ns > 0) {
         TABI_K(K_LU_UPDATE, s);
-        lu_update_kernel<<<nu, kUT, 0, s>>>(H.pc_items.p + uoff[st], k0, T.d_leaf_rng.p,
-                                            T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
+        lu_strip_kernel<<<ns, kUT, 0, s>>>(H.pc_items.p + soff[st], k0, T.d_leaf_rng.p,
+                                           T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
+      }
+      if (ng > 0) {
+        TABI_K(K_LU_UPDATE, s);
+        lu_gemm_kernel<<<ng, kUT, 0, s>>>(H.pc_gitems.p + goff[st], k0, T.d_leaf_rng.p,
+                                          T.d_blk_off.p, T.d_lu.p);
       }
     }
     if (any_big) {

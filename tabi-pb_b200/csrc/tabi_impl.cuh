@@ -267,7 +267,7 @@ struct Handle {
   DBuf<int64_t> ls_bsum, ls_foff, ls_noff;
   DBuf<int2> pc_tiles;
   DBuf<int> pc_info, pc_list;
-  DBuf<int3> pc_items;
+  DBuf<int4> pc_items, pc_gitems;
   DBuf<int2> pc_dblocks;
   // staging of the host-array entry points and of tabi_run_dev
   DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;
