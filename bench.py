@@ -256,6 +256,49 @@ def gpu_arm(args):
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
 
+    # ---- the same solve with the mixed-precision operator (FP32 treecode,
+    # FP64 refinement): same workload, tol, flush and timing
+    mixed = None
+    if not args.no_mixed:
+        msolver = tabipb.TabiSolver(order=w["order"], maxparnode=w["maxparnode"],
+                                    theta=w["theta"], kappa=kap, eps0=w["eps0"], eps1=w["eps1"],
+                                    tol=w["tol"], precision=tabipb.PREC_MIXED)
+
+        def mstep():
+            return msolver.run_dev(nspt, d["sptpos"].data_ptr(), d["sptnrm"].data_ptr(), nface,
+                                   d["nvert"].data_ptr(), natm, d["chrpos"].data_ptr(),
+                                   d["atmchr"].data_ptr(), None, sp)
+
+        for _ in range(args.warmup):
+            mres = mstep()
+        torch.cuda.synchronize()
+        msolver.profile(True)
+        mtimes = []
+        for _ in range(args.steps):
+            flush.zero_()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            mres = mstep()
+            e1.record(stream)
+            mtimes.append((e0, e1))
+        torch.cuda.synchronize()
+        mms = sum(a.elapsed_time(b) for a, b in mtimes)
+        mprof = msolver.profile_read()
+        msolver.close()
+        mms_t = torch.tensor([mms], dtype=torch.float64, device=dev)
+        if world > 1:
+            dist.all_reduce(mms_t, op=dist.ReduceOp.MAX)
+        mms = float(mms_t.item())
+        mixed = {"value": world * args.steps / (mms / 1e3), "unit": "solves/s",
+                 "ms_per_step": mms / args.steps, "gmres_iterations": mres["iter"],
+                 "fp64_residual_measure": mres["err"], "ierr": mres["ierr"],
+                 "soleng_kcal_mol": mres["soleng"],
+                 "dG_rel_diff_vs_fp64": abs(mres["soleng"] - res["soleng"]) / abs(res["soleng"]),
+                 "phase_ms_per_step": {k: v[0] / args.steps for k, v in mprof.items()
+                                       if k != "all"},
+                 "gpu_launches": int(mprof["all"][1])}
+
     # ---- end to end through the host-array C ABI: one handle (one molecule
     # at a time, buffers reused), host arrays in and out every step
     e2e_steps = max(1, min(args.steps, 3))
@@ -343,6 +386,8 @@ def gpu_arm(args):
             "gpu_launches": int(prof["all"][1]),
             "clocks": clk,
         }
+        if mixed is not None:
+            out["mixed"] = mixed
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -399,6 +444,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("gpu", "reference"), default="gpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision leg (FP32 treecode + FP64 refinement)")
     ap.add_argument("--iters", type=int, default=27,
                     help="GMRES iterations used to scale the reference-arm sample")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="globular")

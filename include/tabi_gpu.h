@@ -40,6 +40,14 @@ extern "C" {
 #define TABI_ERR_LIMIT (-6)     /* an internal size limit was exceeded */
 
 #define TABI_PREC_FP64 0 /* plain FP64 treecode (the reference's arithmetic) */
+/* Mixed precision (no counterpart in the reference): the treecode operator
+ * (moments contraction, Taylor recurrences, near-field kernels, per-leaf and
+ * per-cluster sums) in FP32, the per-target sum over leaves and clusters in
+ * FP64; tabi_matvec applies that FP32 operator.  tabi_solve wraps GMRES on it
+ * in FP64 iterative refinement: the residual b - A x with the FP64 operator,
+ * the preconditioner (FP64 leaf LU), Arnoldi, Givens and the energy stay FP64,
+ * and the stopping test is the FP64 |M^-1 (b - A x)| / |M^-1 b| <= tol. */
+#define TABI_PREC_MIXED 1
 
 typedef struct tabi_handle_s* tabi_h;
 

@@ -166,7 +166,7 @@ void givens(double t1, double t2, double& c, double& s) {
 }  // namespace
 
 void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err_out,
-               int* ierr_out, double* hist, int* nhist, cudaStream_t s) {
+               int* ierr_out, double* hist, int* nhist, cudaStream_t s, double tol_in) {
   const int n = 2 * H.n;
   int maxl = H.prm.maxl;
   if (maxl == 0) maxl = 10;
@@ -176,7 +176,7 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
   int nrmax = H.prm.nrmax;
   if (nrmax == 0) nrmax = 10;
   if (nrmax == -1) nrmax = 0;
-  double tol = H.prm.tol;
+  double tol = tol_in >= 0.0 ? tol_in : H.prm.tol;
   if (tol == 0.0) tol = 500 * 1e-20;
   const int maxlp1 = maxl + 1, ldh = maxlp1;
   H.d_v.alloc((size_t)n * maxlp1);
@@ -384,6 +384,88 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
     ierr = 2;
     break;
   }
+  TABI_CUDA(cudaStreamSynchronize(s));
+  TABI_CUDA(cudaGetLastError());
+  *iter_out = iter;
+  *err_out = err;
+  *ierr_out = ierr;
+  if (nhist) *nhist = nh;
+}
+
+// Mixed precision: FP64 iterative refinement around GMRES on the FP32
+// treecode operator.  Each outer step forms the true residual r = b - A x with
+// the FP64 operator and measures it the way DGMRES does for ITOL = 2,
+// |M^-1 r| / |M^-1 b|; while that is above tol, GMRES (FP64 vectors, Arnoldi
+// and Givens, FP32 operator) solves A d = r to the relative tolerance
+// tol * |M^-1 b| / |M^-1 r| and x += d.  The FP64 residual is the judge: the
+// solve stops only when it is below tol.  iter counts the inner iterations,
+// err is the final FP64 measure, err_hist the inner estimates rescaled to
+// |M^-1 b| (at most (nrmax+1)*maxl of them, the same cap as the FP64 path,
+// which also bounds the inner iterations in total).
+void solve_dev(Handle& H, const double* b, double* x, int* iter_out, double* err_out,
+               int* ierr_out, double* hist, int* nhist, cudaStream_t s) {
+  if (H.prm.precision != TABI_PREC_MIXED) {
+    H.mv_prec = TABI_PREC_FP64;
+    gmres_dev(H, b, x, iter_out, err_out, ierr_out, hist, nhist, s);
+    return;
+  }
+  const int n = 2 * H.n;
+  int maxl = H.prm.maxl == 0 ? 10 : H.prm.maxl;
+  int nrmax = H.prm.nrmax == 0 ? 10 : (H.prm.nrmax == -1 ? 0 : H.prm.nrmax);
+  const int cap = (nrmax + 1) * maxl;
+  double tol = H.prm.tol;
+  if (tol == 0.0) tol = 500 * 1e-20;
+  H.d_ir_r.alloc(n);
+  H.d_ir_d.alloc(n);
+  H.d_ir_t.alloc(n);
+  double* r = H.d_ir_r.p;
+  double* d = H.d_ir_d.p;
+  double* t = H.d_ir_t.p;
+  const int vb = kVecBlocks, vt = 256;
+  msolve_dev(H, b, t, s);
+  const double bnrm = nrm2_dev(H, t, n, s);
+  std::vector<double> inner_hist((size_t)cap + 1);
+  int iter = 0, ierr = 0, nh = 0;
+  double err = 0.0;
+  constexpr int kMaxOuter = 20;
+  for (int outer = 0;; ++outer) {
+    // FP64 residual and its ITOL = 2 measure
+    H.mv_prec = TABI_PREC_FP64;
+    matvec_dev(H, x, r, s, true);
+    { TABI_K(K_VEC, s); sub_kernel<<<vb, vt, 0, s>>>(n, b, r); }
+    msolve_dev(H, r, t, s);
+    err = nrm2_dev(H, t, n, s) / bnrm;
+    if (err <= tol) {
+      ierr = 0;
+      break;
+    }
+    if (outer == kMaxOuter || iter >= cap) {
+      ierr = 1;
+      break;
+    }
+    // inner GMRES on the FP32 operator: A d = r from d = 0
+    H.mv_prec = TABI_PREC_MIXED;
+    TABI_CUDA(cudaMemsetAsync(d, 0, sizeof(double) * n, s));
+    int it = 0, ie = 0, nhi = 0;
+    double ei = 0.0;
+    gmres_dev(H, r, d, &it, &ei, &ie, inner_hist.data(), &nhi, s, tol / err);
+    for (int k = 0; k < nhi && nh < cap; ++k) {
+      if (hist) hist[nh] = inner_hist[k] * err;
+      ++nh;
+    }
+    iter += it;
+    { TABI_K(K_VEC, s); axpy_kernel<<<vb, vt, 0, s>>>(n, 1.0, d, x); }
+    if (ie == 2 || ie < 0) {  // stagnation (or an input error) of the inner solve
+      H.mv_prec = TABI_PREC_FP64;
+      matvec_dev(H, x, r, s, true);
+      { TABI_K(K_VEC, s); sub_kernel<<<vb, vt, 0, s>>>(n, b, r); }
+      msolve_dev(H, r, t, s);
+      err = nrm2_dev(H, t, n, s) / bnrm;
+      ierr = err <= tol ? 0 : ie;
+      break;
+    }
+  }
+  H.mv_prec = TABI_PREC_MIXED;
   TABI_CUDA(cudaStreamSynchronize(s));
   TABI_CUDA(cudaGetLastError());
   *iter_out = iter;

@@ -91,9 +91,9 @@ __global__ void mom_partial_kernel(const int4* __restrict__ chunks,
   if (own) mraw[((size_t)ch.w * 4 + set) * NT + term] = acc;
 }
 
-template <int P>
+template <int P, typename TO>
 __global__ void mom_final_kernel(const int2* __restrict__ mslot_chunks,
-                                 const double* __restrict__ mraw, double* __restrict__ mw) {
+                                 const double* __restrict__ mraw, TO* __restrict__ mw) {
   constexpr int NT = tabi_nterms(P);
   int slot = blockIdx.x;
   int2 cr = mslot_chunks[slot];
@@ -112,39 +112,43 @@ __global__ void mom_final_kernel(const int2* __restrict__ mslot_chunks,
     double w = 1.0;
     for (int m = 0; m < 3; ++m)
       for (int j = 1; j <= kk[idx][m]; ++j) w *= (double)(kv[m] + j);
-    mw[(size_t)slot * 16 * NT + q] = sgn * w * raw;
+    mw[(size_t)slot * 16 * NT + q] = (TO)(sgn * w * raw);
   }
 }
 
 // ---- far field
-template <int P>
+// T = double: the reference's arithmetic.  T = float (mixed precision): the
+// target-to-centre offset is formed in FP64 and rounded once, the Taylor
+// recurrences and the contraction run in FP32, the result is widened to FP64
+// for the per-target sum.
+template <int P, typename T>
 __global__ void __launch_bounds__(64) far_kernel(const WorkItem* __restrict__ work,
                                                  const int2* __restrict__ ent,
-                                                 const double* __restrict__ mw,
+                                                 const T* __restrict__ mw,
                                                  const double* __restrict__ nd_mid,
                                                  const double* __restrict__ px,
                                                  const double* __restrict__ py,
                                                  const double* __restrict__ pz,
                                                  const double* __restrict__ nx,
                                                  const double* __restrict__ ny,
-                                                 const double* __restrict__ nz, double kappa,
-                                                 double eps, double2* __restrict__ res) {
+                                                 const double* __restrict__ nz, T kappa,
+                                                 T eps, double2* __restrict__ res) {
   constexpr int NT = tabi_nterms(P);
-  __shared__ double smw[16 * NT];
+  __shared__ T smw[16 * NT];
   WorkItem wi = work[blockIdx.x];
-  const double* src = mw + (size_t)wi.mslot * 16 * NT;
+  const T* src = mw + (size_t)wi.mslot * 16 * NT;
   for (int q = threadIdx.x; q < 16 * NT; q += blockDim.x) smw[q] = src[q];
   __syncthreads();
   if ((int)threadIdx.x >= wi.count) return;
   int2 e = ent[wi.start + threadIdx.x];
   int t = e.x;
   // COMP_TCOEFF :707-709: dx = target - mid
-  double dx = px[t] - nd_mid[3 * wi.node];
-  double dy = py[t] - nd_mid[3 * wi.node + 1];
-  double dz = pz[t] - nd_mid[3 * wi.node + 2];
-  double o1, o2;
-  far_eval<P, double>(dx, dy, dz, kappa, smw, nx[t], ny[t], nz[t], eps, 1.0 / eps, o1, o2);
-  res[e.y] = make_double2(o1 * kOneOver4Pi, o2 * kOneOver4Pi);
+  T dx = (T)(px[t] - nd_mid[3 * wi.node]);
+  T dy = (T)(py[t] - nd_mid[3 * wi.node + 1]);
+  T dz = (T)(pz[t] - nd_mid[3 * wi.node + 2]);
+  T o1, o2;
+  far_eval<P, T>(dx, dy, dz, kappa, smw, (T)nx[t], (T)ny[t], (T)nz[t], eps, T(1) / eps, o1, o2);
+  res[e.y] = make_double2((double)o1 * kOneOver4Pi, (double)o2 * kOneOver4Pi);
 }
 
 // ---- near field
@@ -215,6 +219,109 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel(
   if (own) res[slot] = make_double2(p1, p2);
 }
 
+// Mixed-precision near field.  Each face's position relative to the centre of
+// its leaf is kept as an unevaluated FP32 sum hi + lo (to ~2^-48 of the leaf
+// size), with its area and its normal in FP32 (leaf_rel_kernel, once per tree);
+// the target is split the same way against the same centre.  r - s is then
+// (hi_s - hi_t) + (lo_s - lo_t), accurate to FP32 rounding of |r - s| itself:
+// with one rounded FP32 coordinate, n.(r - s) of adjacent panels (a few
+// hundredths of an Angstrom on a curved surface) would carry the 1e-6 A
+// rounding of leaf-sized coordinates, an error of ~1e-4 relative in K1 and K4.
+// The four kernels and the per-(target, leaf) sum run in FP32; the per-target
+// sum over leaves stays FP64 (reduce_kernel).
+__global__ void leaf_rel_kernel(const int* __restrict__ leaves, const int* __restrict__ nd_ibeg,
+                                const int* __restrict__ nd_num, const double* __restrict__ nd_mid,
+                                const double* __restrict__ px, const double* __restrict__ py,
+                                const double* __restrict__ pz, const double* __restrict__ nx,
+                                const double* __restrict__ ny, const double* __restrict__ nz,
+                                const double* __restrict__ area, float4* __restrict__ lpos,
+                                float4* __restrict__ llo, float4* __restrict__ lnrm) {
+  const int node = leaves[blockIdx.x];
+  const int ib = nd_ibeg[node], m = nd_num[node];
+  const double mx = nd_mid[3 * node], my = nd_mid[3 * node + 1], mz = nd_mid[3 * node + 2];
+  for (int q = threadIdx.x; q < m; q += blockDim.x) {
+    const int j = ib + q;
+    const double rx = px[j] - mx, ry = py[j] - my, rz = pz[j] - mz;
+    const float hx = (float)rx, hy = (float)ry, hz = (float)rz;
+    lpos[j] = make_float4(hx, hy, hz, (float)area[j]);
+    llo[j] = make_float4((float)(rx - hx), (float)(ry - hy), (float)(rz - hz), 0.f);
+    lnrm[j] = make_float4((float)nx[j], (float)ny[j], (float)nz[j], 0.f);
+  }
+}
+
+constexpr int kNearTileF = 256;
+
+__global__ void __launch_bounds__(kNearThreads) near_kernel_f32(
+    const WorkItem* __restrict__ work, const int2* __restrict__ ent,
+    const int* __restrict__ nd_ibeg, const int* __restrict__ nd_num,
+    const double* __restrict__ nd_mid, const double* __restrict__ px,
+    const double* __restrict__ py, const double* __restrict__ pz,
+    const float4* __restrict__ lpos, const float4* __restrict__ llo,
+    const float4* __restrict__ lnrm, const double* __restrict__ x, int n, float kappa,
+    float eps, double2* __restrict__ res) {
+  __shared__ float4 s_p[kNearTileF];  // relative position (hi), A * x1
+  __shared__ float4 s_l[kNearTileF];  // relative position (lo)
+  __shared__ float4 s_n[kNearTileF];  // normal, A * x2
+  WorkItem wi = work[blockIdx.x];
+  const int ib = nd_ibeg[wi.node], nsrc = nd_num[wi.node];
+  const bool own = (int)threadIdx.x < wi.count;
+  int t = 0, slot = 0;
+  float tx = 0.f, ty = 0.f, tz = 0.f, lx = 0.f, ly = 0.f, lz = 0.f;
+  float vx = 0.f, vy = 0.f, vz = 0.f;
+  if (own) {
+    int2 e = ent[wi.start + threadIdx.x];
+    t = e.x;
+    slot = e.y;
+    const double rx = px[t] - nd_mid[3 * wi.node];
+    const double ry = py[t] - nd_mid[3 * wi.node + 1];
+    const double rz = pz[t] - nd_mid[3 * wi.node + 2];
+    tx = (float)rx;
+    ty = (float)ry;
+    tz = (float)rz;
+    lx = (float)(rx - tx);
+    ly = (float)(ry - ty);
+    lz = (float)(rz - tz);
+    float4 nv = lnrm[t];
+    vx = nv.x;
+    vy = nv.y;
+    vz = nv.z;
+  }
+  const float inv_eps = 1.f / eps;
+  float p1 = 0.f, p2 = 0.f;
+  for (int b0 = 0; b0 < nsrc; b0 += kNearTileF) {
+    const int cnt = min(kNearTileF, nsrc - b0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+      const int j = ib + b0 + q;
+      float4 a = lpos[j], b = lnrm[j];
+      const double A = (double)a.w;
+      a.w = (float)(A * x[j]);
+      b.w = (float)(A * x[n + j]);
+      s_p[q] = a;
+      s_l[q] = llo[j];
+      s_n[q] = b;
+    }
+    __syncthreads();
+    if (own) {
+      const int self = t - (ib + b0);
+#pragma unroll 4
+      for (int q = 0; q < cnt; ++q) {
+        const float4 a = s_p[q], l = s_l[q], b = s_n[q];
+        const bool skip = (q == self);
+        float dx = (a.x - tx) + (l.x - lx), dy = (a.y - ty) + (l.y - ly),
+              dz = (a.z - tz) + (l.z - lz);
+        if (skip) dx = 1.f;  // keeps the skipped pair finite
+        float K1, K2, K3, K4;
+        bie4(dx, dy, dz, vx, vy, vz, b.x, b.y, b.z, kappa, eps, inv_eps, K1, K2, K3, K4);
+        const float w1 = skip ? 0.f : a.w, w2 = skip ? 0.f : b.w;
+        p1 = fmaf(K1, w1, fmaf(K2, w2, p1));
+        p2 = fmaf(K3, w1, fmaf(K4, w2, p2));
+      }
+    }
+  }
+  if (own) res[slot] = make_double2((double)p1, (double)p2);
+}
+
 __global__ void reduce_kernel(const int64_t* __restrict__ slot_off,
                               const double2* __restrict__ res, const double* __restrict__ x,
                               int n, double pre1, double pre2, double* __restrict__ y) {
@@ -231,7 +338,7 @@ __global__ void reduce_kernel(const int64_t* __restrict__ slot_off,
 }
 
 template <int P>
-void launch_moments(Handle& H, const double* x, cudaStream_t s) {
+void launch_moments(Handle& H, const double* x, bool f32, cudaStream_t s) {
   Tree& T = H.tree;
   constexpr int NT = tabi_nterms(P);
   if (T.nmslot == 0) return;
@@ -244,20 +351,50 @@ void launch_moments(Handle& H, const double* x, cudaStream_t s) {
                                                   H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p, H.d_ny.p,
                                                   H.d_nz.p, H.d_area.p, x, H.n, H.d_mraw.p);
   }
-  {
-    TABI_K(K_MOMENTS, s);
-    mom_final_kernel<P><<<T.nmslot, 256, 0, s>>>(T.d_mslot_chunks.p, H.d_mraw.p, H.d_mw.p);
-  }
+  TABI_K(K_MOMENTS, s);
+  if (f32)
+    mom_final_kernel<P, float><<<T.nmslot, 256, 0, s>>>(T.d_mslot_chunks.p, H.d_mraw.p,
+                                                          H.d_mwf.p);
+  else
+    mom_final_kernel<P, double><<<T.nmslot, 256, 0, s>>>(T.d_mslot_chunks.p, H.d_mraw.p,
+                                                           H.d_mw.p);
 }
 
 template <int P>
-void launch_far(Handle& H, cudaStream_t s) {
+void launch_far(Handle& H, bool f32, cudaStream_t s) {
   Tree& T = H.tree;
   if (T.far_work.empty()) return;
+  const double eps = H.prm.eps1 / H.prm.eps0;
   TABI_K(K_FAR, s);
-  far_kernel<P><<<(int)T.far_work.size(), 64, 0, s>>>(
-      T.d_far_work.p, T.d_far_ent.p, H.d_mw.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p,
-      H.d_ny.p, H.d_nz.p, H.prm.kappa, H.prm.eps1 / H.prm.eps0, H.d_res.p);
+  if (f32)
+    far_kernel<P, float><<<(int)T.far_work.size(), 64, 0, s>>>(
+        T.d_far_work.p, T.d_far_ent.p, H.d_mwf.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p,
+        H.d_nx.p, H.d_ny.p, H.d_nz.p, (float)H.prm.kappa, (float)eps, H.d_res.p);
+  else
+    far_kernel<P, double><<<(int)T.far_work.size(), 64, 0, s>>>(
+        T.d_far_work.p, T.d_far_ent.p, H.d_mw.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p,
+        H.d_nx.p, H.d_ny.p, H.d_nz.p, H.prm.kappa, eps, H.d_res.p);
+}
+
+// FP32 copies of the faces relative to their leaf centres (once per tree)
+void prepare_f32(Handle& H, cudaStream_t s) {
+  Tree& T = H.tree;
+  if (T.lrel_ready) return;
+  T.d_leaves.alloc(std::max(T.nleaf, 1));
+  TABI_CUDA(cudaMemcpyAsync(T.d_leaves.p, T.leaves.data(), sizeof(int) * T.nleaf,
+                            cudaMemcpyHostToDevice, s));
+  T.d_lpos.alloc(std::max(H.n, 1));
+  T.d_llo.alloc(std::max(H.n, 1));
+  T.d_lnrm.alloc(std::max(H.n, 1));
+  {
+    TABI_K(K_TREE, s);
+    leaf_rel_kernel<<<T.nleaf, 256, 0, s>>>(T.d_leaves.p, T.d_ibeg.p, T.d_num.p, T.d_mid.p,
+                                            H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p, H.d_ny.p,
+                                            H.d_nz.p, H.d_area.p, T.d_lpos.p, T.d_llo.p,
+                                            T.d_lnrm.p);
+  }
+  TABI_CUDA(cudaGetLastError());
+  T.lrel_ready = true;
 }
 
 }  // namespace
@@ -301,6 +438,11 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
     }
   }
   Tree& T = H.tree;
+  const bool f32 = H.mv_prec == TABI_PREC_MIXED;
+  if (f32) {
+    prepare_f32(H, s);
+    if (T.nmslot > 0) H.d_mwf.alloc(H.d_mw.n);
+  }
   TABI_PHASE(K_PHASE_MATVEC, s);
   // the near field runs on the handle's side stream, concurrently with the
   // moments + far field on s; both write disjoint result slots
@@ -313,17 +455,23 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
   // moments first (small, needed by the far field), then the near field on
   // the side stream and the far field on s
   switch (H.prm.order) {
-    case 1: launch_moments<1>(H, x, s); break;
-    case 2: launch_moments<2>(H, x, s); break;
-    case 3: launch_moments<3>(H, x, s); break;
-    case 4: launch_moments<4>(H, x, s); break;
-    case 5: launch_moments<5>(H, x, s); break;
-    case 6: launch_moments<6>(H, x, s); break;
-    case 7: launch_moments<7>(H, x, s); break;
-    case 8: launch_moments<8>(H, x, s); break;
+    case 1: launch_moments<1>(H, x, f32, s); break;
+    case 2: launch_moments<2>(H, x, f32, s); break;
+    case 3: launch_moments<3>(H, x, f32, s); break;
+    case 4: launch_moments<4>(H, x, f32, s); break;
+    case 5: launch_moments<5>(H, x, f32, s); break;
+    case 6: launch_moments<6>(H, x, f32, s); break;
+    case 7: launch_moments<7>(H, x, f32, s); break;
+    case 8: launch_moments<8>(H, x, f32, s); break;
     default: throw Error(TABI_ERR_ARG, "order must be 1..8");
   }
-  if (!T.near_work.empty()) {
+  if (!T.near_work.empty() && f32) {
+    TABI_K(K_NEAR, sn);
+    near_kernel_f32<<<(int)T.near_work.size(), kNearThreads, 0, sn>>>(
+        T.d_near_work.p, T.d_near_ent.p, T.d_ibeg.p, T.d_num.p, T.d_mid.p, H.d_x.p, H.d_y.p,
+        H.d_z.p, T.d_lpos.p, T.d_llo.p, T.d_lnrm.p, x, n, (float)H.prm.kappa,
+        (float)(H.prm.eps1 / H.prm.eps0), H.d_res.p);
+  } else if (!T.near_work.empty()) {
     TABI_K(K_NEAR, sn);
     near_kernel<<<(int)T.near_work.size(), kNearThreads, 0, sn>>>(
         T.d_near_work.p, T.d_near_ent.p, T.d_ibeg.p, T.d_num.p, H.d_x.p, H.d_y.p, H.d_z.p,
@@ -331,14 +479,14 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
         H.d_res.p);
   }
   switch (H.prm.order) {
-    case 1: launch_far<1>(H, s); break;
-    case 2: launch_far<2>(H, s); break;
-    case 3: launch_far<3>(H, s); break;
-    case 4: launch_far<4>(H, s); break;
-    case 5: launch_far<5>(H, s); break;
-    case 6: launch_far<6>(H, s); break;
-    case 7: launch_far<7>(H, s); break;
-    case 8: launch_far<8>(H, s); break;
+    case 1: launch_far<1>(H, f32, s); break;
+    case 2: launch_far<2>(H, f32, s); break;
+    case 3: launch_far<3>(H, f32, s); break;
+    case 4: launch_far<4>(H, f32, s); break;
+    case 5: launch_far<5>(H, f32, s); break;
+    case 6: launch_far<6>(H, f32, s); break;
+    case 7: launch_far<7>(H, f32, s); break;
+    case 8: launch_far<8>(H, f32, s); break;
     default: break;
   }
   if (fork) {

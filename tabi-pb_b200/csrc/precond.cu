@@ -680,7 +680,7 @@ __global__ void lu_diaginv_kernel(const int2* __restrict__ blocks,  // (leaf, k0
 // and the rows below (above) are updated with a 32-wide GEMV by all threads.
 // Large blocks run with 512 threads; leaf_list selects the launch's leaves.
 template <int NT>
-__global__ void __launch_bounds__(NT, 1) solve_kernel(
+__global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     const int2* __restrict__ leaf_rng, const int64_t* __restrict__ blk_off,
     const int64_t* __restrict__ dinv_off, const int* __restrict__ leaf_list,
     const double* __restrict__ lu, const double* __restrict__ dinv,
@@ -928,11 +928,13 @@ void build_precond(Handle& H, cudaStream_t s) {
     { TABI_K(K_LU_POST, s); lu_diaginv_kernel<<<(int)(dblocks.size() / 4), 128, 0, s>>>(
         H.pc_dblocks.p, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_lu.p, T.d_dinv.p); }
   }
-  // apply lists: blocks of order > 256 (largest first) get 512 threads
+  // apply lists: blocks of order > 512 get 512 threads (one wave on the GPU),
+  // the others 256 threads on the side stream; largest first in each
   {
     std::vector<int> big, small;
-    for (int l = 0; l < nl; ++l) (2 * rng[l].y > 256 ? big : small).push_back(l);
+    for (int l = 0; l < nl; ++l) (2 * rng[l].y > 512 ? big : small).push_back(l);
     std::sort(big.begin(), big.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
+    std::sort(small.begin(), small.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
     T.n_solve_big = (int)big.size();
     T.n_solve_small = (int)small.size();
     big.insert(big.end(), small.begin(), small.end());
@@ -962,6 +964,12 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
     TABI_CUDA(cudaFuncSetAttribute(solve_kernel<512>,
                                    cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   }
+  const bool fork = T.n_solve_big > 0 && T.n_solve_small > 0 && H.side != nullptr;
+  cudaStream_t s2 = fork ? H.side : s;
+  if (fork) {
+    TABI_CUDA(cudaEventRecord(H.ev_fork, s));
+    TABI_CUDA(cudaStreamWaitEvent(s2, H.ev_fork, 0));
+  }
   if (T.n_solve_big > 0) {
     TABI_K(K_SOLVE, s);
     solve_kernel<512><<<T.n_solve_big, 512, smem, s>>>(
@@ -969,10 +977,14 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
         T.d_lu_perm.p, n, r, z);
   }
   if (T.n_solve_small > 0) {
-    TABI_K(K_SOLVE, s);
-    solve_kernel<256><<<T.n_solve_small, 256, smem, s>>>(
+    TABI_K(K_SOLVE, s2);
+    solve_kernel<256><<<T.n_solve_small, 256, smem, s2>>>(
         T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_solve_list.p + T.n_solve_big,
         T.d_lu.p, T.d_dinv.p, T.d_lu_perm.p, n, r, z);
+  }
+  if (fork) {
+    TABI_CUDA(cudaEventRecord(H.ev_join, s2));
+    TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
   }
   TABI_CUDA(cudaGetLastError());
 }

@@ -132,7 +132,8 @@ void check_params(const tabi_params& p) {
   TABI_REQUIRE(p.maxl >= 0 && p.maxl <= 60, TABI_ERR_ARG, "maxl must be in 0..60");
   TABI_REQUIRE(p.nrmax >= -1, TABI_ERR_ARG, "nrmax must be >= -1");
   TABI_REQUIRE(p.tol >= 0.0, TABI_ERR_ARG, "tol must be >= 0");
-  TABI_REQUIRE(p.precision == TABI_PREC_FP64, TABI_ERR_ARG, "unsupported precision mode");
+  TABI_REQUIRE(p.precision == TABI_PREC_FP64 || p.precision == TABI_PREC_MIXED, TABI_ERR_ARG,
+               "precision must be TABI_PREC_FP64 or TABI_PREC_MIXED");
   TABI_REQUIRE(p.maxparnode <= 12000, TABI_ERR_LIMIT, "maxparnode above 12000");
 }
 
@@ -189,6 +190,7 @@ int tabi_create(tabi_h* h, const tabi_params* p) {
     TABI_REQUIRE(ndev > 0, TABI_ERR_CUDA, "no CUDA device");
     nh = new tabi_handle_s();
     nh->H.prm = *p;
+    nh->H.mv_prec = p->precision;
     TABI_CUDA(cudaGetDevice(&nh->H.device));
     TABI_CUDA(cudaStreamCreateWithFlags(&nh->H.stream, cudaStreamNonBlocking));
     TABI_CUDA(cudaStreamCreateWithFlags(&nh->H.side, cudaStreamNonBlocking));
@@ -401,7 +403,7 @@ int tabi_solve_dev(tabi_h h, int n2, const double* b_dev, double* x_dev, int* it
     require_tree(H, n2);
     TABI_REQUIRE(b_dev && x_dev && iter && err && ierr, TABI_ERR_ARG, "null argument");
     set_device(H);
-    gmres_dev(H, b_dev, x_dev, iter, err, ierr, err_hist, n_hist, pick(H, stream));
+    solve_dev(H, b_dev, x_dev, iter, err, ierr, err_hist, n_hist, pick(H, stream));
   });
 }
 
@@ -418,7 +420,7 @@ int tabi_solve(tabi_h h, int n2, const double* b, double* x, int* iter, double* 
     H.d_xio.alloc(n2);
     TABI_CUDA(cudaMemcpyAsync(H.d_b.p, b, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
     TABI_CUDA(cudaMemcpyAsync(H.d_xio.p, x, sizeof(double) * n2, cudaMemcpyHostToDevice, s));
-    gmres_dev(H, H.d_b.p, H.d_xio.p, iter, err, ierr, err_hist, n_hist, s);
+    solve_dev(H, H.d_b.p, H.d_xio.p, iter, err, ierr, err_hist, n_hist, s);
     TABI_CUDA(cudaMemcpyAsync(x, H.d_xio.p, sizeof(double) * n2, cudaMemcpyDeviceToHost, s));
     TABI_CUDA(cudaStreamSynchronize(s));
   });
@@ -526,7 +528,7 @@ int tabi_run_dev(tabi_h h, int nspt, const double* sptpos_dev, const double* spt
     TABI_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * 2 * nface, s));
     int iter = 0, ierr = 0;
     double err = 0.0, se = 0.0, ce = 0.0;
-    gmres_dev(H, b.p, x, &iter, &err, &ierr, nullptr, nullptr, s);
+    solve_dev(H, b.p, x, &iter, &err, &ierr, nullptr, nullptr, s);
     mark("gmres");
     energy_dev(H, nchr, nullptr, nullptr, x, &se, &ce, s);
     mark("energy");

@@ -98,6 +98,7 @@ struct Tree {
     dinv_off.clear();
     n_solve_big = n_solve_small = 0;
     max_leaf = 0;
+    lrel_ready = false;
   }
   int n = 0;          // faces
   int nnodes = 0;
@@ -137,6 +138,12 @@ struct Tree {
   DBuf<int> d_lu_perm;           // per leaf row permutation of all pivots
   int n_solve_big = 0, n_solve_small = 0;
   int max_leaf = 0;
+  // mixed precision: leaf ids on the device; each face relative to its leaf
+  // centre as FP32 hi + lo (with its area in lpos.w) and its normal in FP32
+  // (built on first use)
+  DBuf<int> d_leaves;
+  DBuf<float4> d_lpos, d_llo, d_lnrm;
+  bool lrel_ready = false;
 };
 
 // Kernel classes for the launch counters / event timers (tabi_profile_*).
@@ -240,6 +247,8 @@ struct Handle {
   // matvec scratch
   DBuf<double> d_mraw;    // moment partials
   DBuf<double> d_mw;      // weighted moments, 16 x NT per slot
+  DBuf<float> d_mwf;      // the same in FP32 (mixed-precision far field)
+  int mv_prec = TABI_PREC_FP64;  // arithmetic of the treecode operator
   DBuf<double2> d_res;    // per-slot interaction results
   DBuf<double> d_red;     // reduction scratch
   DBuf<double> h_red_pinned_dummy;
@@ -247,6 +256,7 @@ struct Handle {
   // GMRES workspace
   DBuf<double> d_v, d_wk, d_dl, d_gz, d_r, d_b, d_xio, d_tmp;
   DBuf<double> d_coef, d_orth;
+  DBuf<double> d_ir_r, d_ir_d, d_ir_t;  // mixed-precision refinement
   // energy scratch
   DBuf<double> d_ptl;
   DBuf<double> d_atoms;
@@ -294,6 +304,10 @@ void build_precond(Handle& H, cudaStream_t s);
 void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s);
 // gmres (gmres.cu)
 void gmres_dev(Handle& H, const double* b, double* x, int* iter, double* err, int* ierr,
+               double* hist, int* nhist, cudaStream_t s, double tol = -1.0);
+// the solve the handle's precision asks for: gmres_dev (FP64) or FP64 GMRES-IR
+// around FP32-operator GMRES (mixed)
+void solve_dev(Handle& H, const double* b, double* x, int* iter, double* err, int* ierr,
                double* hist, int* nhist, cudaStream_t s);
 double dot_dev(Handle& H, const double* a, const double* b, int n, cudaStream_t s);
 double nrm2_dev(Handle& H, const double* a, int n, cudaStream_t s);

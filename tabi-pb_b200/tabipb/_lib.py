@@ -33,6 +33,10 @@ SYMBOLS = [
 ]
 
 
+PREC_FP64 = 0   # TABI_PREC_FP64: the reference's FP64 arithmetic
+PREC_MIXED = 1  # TABI_PREC_MIXED: FP32 treecode operator, FP64 refinement
+
+
 class TabiError(RuntimeError):
     def __init__(self, code, msg):
         super().__init__(f"{TABI_ERRORS.get(code, code)}: {msg}")
