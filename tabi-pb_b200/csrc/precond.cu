@@ -674,11 +674,23 @@ __global__ void lu_diaginv_kernel(const int2* __restrict__ blocks,  // (leaf, k0
   for (int i = 0; i < kDB; ++i) Ui[(size_t)lane * kDB + i] = x[i];
 }
 
+// L2 prefetch of a byte range (bulk, no completion to wait for); the range
+// starts 16-byte aligned and is a multiple of 16 bytes long, which holds for
+// every column segment of a factor block (even order, offsets of 32 rows).
+__device__ __forceinline__ void prefetch_l2(const double* p, int ndouble) {
+  if (ndouble > 0)
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p),
+                 "r"((unsigned)ndouble * 8u)
+                 : "memory");
+}
+
 // Forward/back substitution with the factored block (DGETRS 'N') in 32-row
 // steps: gather through the pivot permutation, then per step the diagonal
 // block is applied as a 32 x 32 GEMV with its precomputed inverse (one warp)
 // and the rows below (above) are updated with a 32-wide GEMV by all threads.
-// Large blocks run with 512 threads; leaf_list selects the launch's leaves.
+// The steps form a dependent chain, so each one's column panel and inverse
+// block are prefetched into L2 kPF steps ahead (by warp 1).  Large blocks run
+// with 512 threads; leaf_list selects the launch's leaves.
 template <int NT>
 __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     const int2* __restrict__ leaf_rng, const int64_t* __restrict__ blk_off,
@@ -698,10 +710,27 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     int src = pm[i];
     xs[i] = (src < n) ? r[ib + src] : r[N + ib + src - n];
   }
+  constexpr int kPF = 2;
+  // L panel of step kp: columns kp.., rows below its diagonal block
+  auto pf_lower = [&](int kp) {
+    if (kp >= m) return;
+    if (kp + lane < m) prefetch_l2(A + (size_t)(kp + lane) * m + kp + kDB, m - kp - kDB);
+    if (lane == 0) prefetch_l2(Di + (size_t)(kp / kDB) * 2 * kDB * kDB, kDB * kDB);
+  };
+  // U panel of block bp: columns bp*32.., rows above its diagonal block
+  auto pf_upper = [&](int bp) {
+    if (bp < 0) return;
+    const int kp = bp * kDB;
+    if (kp + lane < m) prefetch_l2(A + (size_t)(kp + lane) * m, kp);
+    if (lane == 0) prefetch_l2(Di + (size_t)bp * 2 * kDB * kDB + kDB * kDB, kDB * kDB);
+  };
+  if (warp == 1)
+    for (int q = 0; q < kPF; ++q) pf_lower(q * kDB);
   __syncthreads();
   // L y = P r
   for (int k0 = 0; k0 < m; k0 += kDB) {
     const int nb = min(kDB, m - k0);
+    if (warp == 1) pf_lower(k0 + kPF * kDB);
     if (warp == 0) {
       const double* Li = Di + (size_t)(k0 / kDB) * 2 * kDB * kDB;
       double v = 0.0;
@@ -730,9 +759,12 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
   }
   // U x = y
   const int nblk = (m + kDB - 1) / kDB;
+  if (warp == 1)
+    for (int q = 0; q < kPF; ++q) pf_upper(nblk - 1 - q);
   for (int b = nblk - 1; b >= 0; --b) {
     const int k0 = b * kDB;
     const int nb = min(kDB, m - k0);
+    if (warp == 1) pf_upper(b - kPF);
     if (warp == 0) {
       const double* Ui = Di + (size_t)b * 2 * kDB * kDB + kDB * kDB;
       double v = 0.0;
