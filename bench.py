@@ -61,14 +61,13 @@ def far_ops(p):
 
 
 def make_inputs():
-    import oracle as O
     from tabipb import surface as S
 
     w = WORKLOAD
     xyz, q, r = S.synthetic_molecule(w["natm"], w["radius"], min_sep=w["min_sep"],
                                      seed=w["seed"])
     pos, nrm, fc, h = S.gaussian_surface(xyz, r, density=w["density"], probe=w["probe"])
-    fc, _ = O.surface_area(pos, fc)  # readin.f90:264-333 face filter
+    fc, _ = S.face_filter(pos, fc)  # readin.f90:264-333
     return dict(sptpos=np.ascontiguousarray(pos), sptnrm=np.ascontiguousarray(nrm),
                 nvert=np.ascontiguousarray(fc, dtype=np.int32),
                 chrpos=np.ascontiguousarray(xyz), atmchr=np.ascontiguousarray(q), grid=h)

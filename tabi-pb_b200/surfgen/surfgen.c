@@ -310,6 +310,71 @@ int sg_gaussian_surface(int natm, const double* xyzr, double probe,
 
 void sg_free(void* p) { free(p); }
 
+/* Random sequential addition over a given stream of candidate points: cand
+ * (ncand x 3) is scanned in order; a candidate is taken when it lies in the
+ * ball |p| <= radius and every point already in pts (the first *placed on
+ * entry, kept) is at distance >= min_sep ((d.d) < min_sep^2 rejects), until
+ * natm points are placed.  A grid of min_sep cells limits the distance
+ * checks to the 27 cells around the candidate.  Returns the number of
+ * candidates consumed, or -1 on bad arguments / allocation failure. */
+int sg_rsa(int natm, double radius, double min_sep, const double* cand, int ncand,
+           double* pts, int* placed) {
+  if (natm <= 0 || radius <= 0.0 || min_sep <= 0.0 || !cand || !pts || !placed) return -1;
+  const double cell = min_sep, s2 = min_sep * min_sep, r2 = radius * radius;
+  const int nc = (int)ceil(2.0 * radius / cell) + 3;
+  if ((double)nc * nc * nc > 6.4e7) return -1;
+  const size_t ncell = (size_t)nc * nc * nc;
+  int* head = (int*)malloc(sizeof(int) * ncell);
+  int* next = (int*)malloc(sizeof(int) * (size_t)natm);
+  if (!head || !next) {
+    free(head);
+    free(next);
+    return -1;
+  }
+  for (size_t c = 0; c < ncell; ++c) head[c] = -1;
+#define SG_CELL(v) ((int)floor(((v) + radius) / cell) + 1)
+  for (int j = 0; j < *placed; ++j) {
+    const double* q = pts + 3 * (size_t)j;
+    size_t c = ((size_t)SG_CELL(q[2]) * nc + SG_CELL(q[1])) * nc + SG_CELL(q[0]);
+    next[j] = head[c];
+    head[c] = j;
+  }
+  int n = *placed, used = 0;
+  for (; used < ncand && n < natm; ++used) {
+    const double* p = cand + 3 * (size_t)used;
+    if ((p[0] * p[0] + p[1] * p[1]) + p[2] * p[2] > r2) continue;
+    const int cx = SG_CELL(p[0]), cy = SG_CELL(p[1]), cz = SG_CELL(p[2]);
+    int ok = 1;
+    for (int z = cz - 1; z <= cz + 1 && ok; ++z)
+      for (int y = cy - 1; y <= cy + 1 && ok; ++y)
+        for (int x = cx - 1; x <= cx + 1 && ok; ++x) {
+          if (x < 0 || y < 0 || z < 0 || x >= nc || y >= nc || z >= nc) continue;
+          for (int j = head[((size_t)z * nc + y) * nc + x]; j >= 0; j = next[j]) {
+            const double* q = pts + 3 * (size_t)j;
+            const double d0 = q[0] - p[0], d1 = q[1] - p[1], d2 = q[2] - p[2];
+            if ((d0 * d0 + d1 * d1) + d2 * d2 < s2) {
+              ok = 0;
+              break;
+            }
+          }
+        }
+    if (!ok) continue;
+    double* o = pts + 3 * (size_t)n;
+    o[0] = p[0];
+    o[1] = p[1];
+    o[2] = p[2];
+    size_t c = ((size_t)cz * nc + cy) * nc + cx;
+    next[n] = head[c];
+    head[c] = n;
+    ++n;
+  }
+#undef SG_CELL
+  free(head);
+  free(next);
+  *placed = n;
+  return used;
+}
+
 int sg_write_msms(const char* prefix, int nvert, const double* vert,
                   int nface, const int* face, int natm, double density,
                   double probe) {

@@ -13,6 +13,13 @@ int sg_gaussian_surface(int natm, const double* xyzr, double probe,
                         int* nvert_out, int** face_out, int* nface_out,
                         double* spacing_out);
 void sg_free(void* p);
+/* Random sequential addition over a stream of candidate points (ncand x 3,
+ * scanned in order): takes candidates inside the ball of `radius` that keep
+ * distance >= min_sep to every point placed so far, until natm are placed.
+ * pts (natm x 3) holds *placed points on entry, which are kept.  Returns the
+ * number of candidates consumed (-1 on bad arguments). */
+int sg_rsa(int natm, double radius, double min_sep, const double* cand, int ncand,
+           double* pts, int* placed);
 /* Writes <prefix>.vert and <prefix>.face in the MSMS layout the reference
  * reads (readin.f90:204-246). */
 int sg_write_msms(const char* prefix, int nvert, const double* vert,

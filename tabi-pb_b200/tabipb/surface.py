@@ -2,6 +2,8 @@
 
 * ``read_pqr``    -- readin.f90:29-86 (atoms read as REAL*4).
 * ``read_msms`` / ``write_msms`` -- the .vert/.face layout of readin.f90:204-246.
+* ``face_filter`` -- readin.f90:264-333 (surface_area): drops faces of area
+  below 1e-5 and faces whose centroid repeats one of the 10 faces before it.
 * ``icosphere``   -- the Born-ion triangulation (icosahedron subdivided ``level``
   times: level 4 gives 5,120 faces / 2,562 vertices, exact unit normals).
 * ``synthetic_molecule`` -- seeded globular molecules (uniform in a sphere,
@@ -138,38 +140,29 @@ def synthetic_molecule(natm, radius, min_sep=2.0, rad_range=(1.5, 2.0), q_sigma=
     integer with the remainder spread evenly.  Returns (xyz, q, r)."""
     rng = np.random.default_rng(seed)
     pts = np.zeros((natm, 3))
-    cell = min_sep
-    grid = {}
-    n = 0
+    # candidates are drawn in batches from a copy of the generator and the
+    # placement (surfgen.c sg_rsa) runs over them in order; the generator then
+    # advances by exactly the candidates consumed, so the stream -- and with it
+    # the molecule, radii and charges -- is the one of drawing one candidate
+    # (3 uniforms) at a time
+    L = _sglib()
+    placed = C.c_int(0)
+    limit = max_tries * max(1, natm // 100)
     tries = 0
-    while n < natm:
-        tries += 1
-        if tries > max_tries * max(1, natm // 100):
-            raise RuntimeError(f"placed only {n} of {natm} atoms at min_sep {min_sep}")
-        p = rng.uniform(-radius, radius, 3)
-        if p @ p > radius * radius:
-            continue
-        key = tuple(np.floor(p / cell).astype(int))
-        ok = True
-        for dx in (-1, 0, 1):
-            for dy in (-1, 0, 1):
-                for dz in (-1, 0, 1):
-                    for j in grid.get((key[0] + dx, key[1] + dy, key[2] + dz), ()):
-                        d = pts[j] - p
-                        if d @ d < min_sep * min_sep:
-                            ok = False
-                            break
-                    if not ok:
-                        break
-                if not ok:
-                    break
-            if not ok:
-                break
-        if not ok:
-            continue
-        pts[n] = p
-        grid.setdefault(key, []).append(n)
-        n += 1
+    batch = max(4096, 64 * natm)
+    while placed.value < natm:
+        if tries >= limit:
+            raise RuntimeError(f"placed only {placed.value} of {natm} atoms at min_sep {min_sep}")
+        tmp = np.random.Generator(np.random.PCG64())
+        tmp.bit_generator.state = rng.bit_generator.state
+        nb = min(batch, limit - tries)
+        cand = np.ascontiguousarray(tmp.uniform(-radius, radius, (nb, 3)))
+        used = L.sg_rsa(natm, float(radius), float(min_sep), cand.ctypes.data, nb, pts.ctypes.data,
+                        C.byref(placed))
+        if used < 0:
+            raise RuntimeError("sg_rsa failed")
+        rng.bit_generator.advance(3 * used)
+        tries += used
     r = rng.uniform(rad_range[0], rad_range[1], natm)
     q = rng.normal(0.0, q_sigma, natm)
     q -= q.mean()
@@ -191,6 +184,9 @@ def _sglib():
                                           C.POINTER(C.c_double)]
         L.sg_gaussian_surface.restype = C.c_int
         L.sg_free.argtypes = [C.c_void_p]
+        L.sg_rsa.argtypes = [C.c_int, C.c_double, C.c_double, C.c_void_p, C.c_int, C.c_void_p,
+                             C.POINTER(C.c_int)]
+        L.sg_rsa.restype = C.c_int
         _sg = L
     return _sg
 
@@ -229,3 +225,30 @@ def gaussian_surface(xyz, r, density=10.0, probe=1.4, blob=0.0, quantize=True):
         pos = np.round(pos, 3)
         nrm = np.round(nrm, 3)
     return pos, nrm, f, h.value
+
+
+def face_filter(sptpos, nvert):
+    """readin.f90:264-333 (surface_area).  A face is dropped when its Heron area
+    (readin.f90:336-340) is below 1e-5 or its centroid lies within
+    sqrt(1e-5) of the centroid of any of the 10 faces before it in the
+    ORIGINAL list (dropped ones included).  nvert: (nface, 3), 1-based.
+    Returns (nvert of the kept faces, total area of all faces)."""
+    sp = np.ascontiguousarray(sptpos, dtype=np.float64).reshape(-1, 3)
+    nv = np.ascontiguousarray(nvert, dtype=np.int32).reshape(-1, 3)
+    p0, p1, p2 = sp[nv[:, 0] - 1], sp[nv[:, 1] - 1], sp[nv[:, 2] - 1]
+    third = 1.0 / 3.0
+    cen = (third * p0 + third * p1) + third * p2  # accumulated in vertex order
+
+    def dist(a, b):
+        d = a - b
+        return np.sqrt((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2])
+
+    aa, bb, cc = dist(p0, p1), dist(p0, p2), dist(p1, p2)
+    s = 0.5 * ((aa + bb) + cc)
+    area = np.sqrt(((s * (s - aa)) * (s - bb)) * (s - cc))
+    alert = np.zeros(len(nv), bool)
+    for k in range(1, 11):
+        d = cen[k:] - cen[:-k]
+        alert[k:] |= ((d[:, 0] * d[:, 0] + d[:, 1] * d[:, 1]) + d[:, 2] * d[:, 2]) < 1e-5
+    keep = ~((area < 1e-5) | alert)
+    return nv[keep].copy(), float(np.sum(area)) if len(area) else 0.0

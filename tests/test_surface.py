@@ -80,3 +80,24 @@ def test_molecule_case_pipeline():
                                    c["atmchr"], EPS0)
     assert (ar > 0).all()
     np.testing.assert_allclose(np.linalg.norm(tq, axis=1), 1.0, atol=1e-12)
+
+
+def test_face_filter_matches_oracle():
+    """tabipb.surface.face_filter (the product's readin.f90:264-333) keeps the
+    same faces as the oracle's restatement, duplicates and slivers included."""
+    import oracle as O
+    from tabipb import surface as S
+
+    xyz, q, r = S.synthetic_molecule(120, 7.0, min_sep=2.0, seed=9)
+    pos, nrm, fc, _ = S.gaussian_surface(xyz, r, density=4.0, probe=1.4)
+    base, _ = S.face_filter(pos, fc)
+    # plant a repeat of face 5 right after it (caught: within the 10 faces
+    # before it), one at the end (not caught: the reference looks back 10
+    # faces only) and a zero-area sliver
+    fc = np.concatenate([fc[:6], fc[5:6], fc[6:], fc[5:6],
+                         np.array([[fc[7, 0], fc[7, 0], fc[7, 1]]])])
+    a, sa = O.surface_area(pos, fc)
+    b, sb = S.face_filter(pos, fc)
+    assert np.array_equal(a, b)
+    assert len(b) == len(base) + 1
+    assert abs(sa - sb) <= 1e-12 * sa
