@@ -210,6 +210,85 @@ const char* tabi_profile_class_name(int kclass);
  * returns the achieved FP64 FLOP/s (2 per FMA). */
 int tabi_probe_fp64_peak(double ms, double* flops);
 
+/* ---- Learned warm start (no counterpart in the reference, which starts
+ * GMRES from zero, main.f90:133).  A rotation- and translation-invariant
+ * point-cloud network over the panels (16 nearest neighbours per panel,
+ * `layers` residual message-passing layers of width `hidden`, bfloat16 weight
+ * matrices with FP32 accumulation) predicts x0 = [phi; dphi/dn] from the
+ * panel geometry and the right-hand side; GMRES on the true residual then
+ * runs from x0, so the prediction changes the iteration count only.  The
+ * network trains on the GPU (its own forward, backward and Adam kernels) on
+ * solutions of this solver.  All surface arrays are device pointers in the
+ * reference's layout (tr_xyz, tr_q 3 x nface, tr_area nface, bvct and x
+ * 2 nface), in any one face order; stream NULL = the network's own stream.
+ * A network object is not thread-safe. */
+typedef struct tabi_ws_s* tabi_ws;
+
+/* hidden: multiple of 32 in 32..256; layers 1..8; deterministic init from
+ * seed (output layer zero: an untrained network predicts x1 = 0, x2 = b2). */
+int tabi_ws_create(tabi_ws* w, int hidden, int layers, unsigned long long seed);
+int tabi_ws_destroy(tabi_ws w);
+/* number of FP32 parameters (-1 for a NULL network) */
+long long tabi_ws_nparams(tabi_ws w);
+/* FP32 master parameters (host arrays of tabi_ws_nparams floats); set also
+ * resets the optimiser state */
+int tabi_ws_get_params(tabi_ws w, float* theta, long long n);
+int tabi_ws_set_params(tabi_ws w, const float* theta, long long n);
+/* x0 (device, 2 nface) = the network's prediction */
+int tabi_ws_predict_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
+                        const double* tr_area, const double* bvct, double* x0,
+                        void* stream);
+/* loss against a solution x_target (device, 2 nface) and, if grad != NULL,
+ * its gradient with respect to the parameters (host, tabi_ws_nparams) */
+int tabi_ws_loss_grad_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
+                          const double* tr_area, const double* bvct,
+                          const double* x_target, double* loss, float* grad,
+                          void* stream);
+/* one Adam step (beta 0.9 / 0.999) on one molecule; *loss (may be NULL) =
+ * the loss before the step */
+int tabi_ws_train_step_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
+                           const double* tr_area, const double* bvct,
+                           const double* x_target, double lr, double* loss,
+                           void* stream);
+/* the network's input: neighbour lists (host, nface x 16) and node features
+ * (host, nface x 8); either may be NULL */
+int tabi_ws_graph_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
+                      const double* tr_area, const double* bvct, int* nbr, float* feat,
+                      void* stream);
+/* attaches a network to a solve handle (NULL detaches): tabi_run_dev then
+ * starts GMRES from the network's prediction instead of zero.  The handle
+ * does not own the network. */
+int tabi_set_warmstart(tabi_h h, tabi_ws w);
+
+/* ---- Batched solves (no counterpart in the reference, which solves one
+ * molecule per run).  One molecule: device inputs as tabi_run_dev takes them,
+ * plus per-molecule overrides of the leaf size and Taylor order (0 = the batch
+ * parameters'), e.g. from an autotuned table. */
+typedef struct {
+  int nspt;
+  const double* sptpos;  /* 3 x nspt */
+  const double* sptnrm;  /* 3 x nspt */
+  int nface;
+  const int* nvert;      /* 3 x nface, 1-based, already face-filtered */
+  int nchr;
+  const double* chrpos;  /* 3 x nchr */
+  const double* atmchr;  /* nchr */
+  int maxparnode;
+  int order;
+} tabi_mol_dev;
+
+#define TABI_BATCH_STATS 12
+/* Solves nmol molecules with nworkers host threads, each owning a handle (and
+ * its two streams) on the current device, so that the latency-bound phases of
+ * one molecule (panel factorisations, triangular solves, GMRES reductions)
+ * overlap the work of others; molecules are taken largest first.  With a
+ * warm-start network each worker uses its own copy.  stats (may be NULL)
+ * receives TABI_BATCH_STATS doubles per molecule, in input order: the 8 of
+ * tabi_run_dev, the molecule's wall time (ms), its completion time since the
+ * batch started (ms), the worker index and the leaf size used. */
+int tabi_batch_run_dev(const tabi_params* p, int nmol, const tabi_mol_dev* mols, tabi_ws ws,
+                       int nworkers, double* stats);
+
 #ifdef __cplusplus
 }
 #endif

@@ -6,9 +6,13 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <atomic>
+#include <memory>
+#include <thread>
 #include <vector>
 
 #include "tabi_impl.cuh"
+#include "warmstart.cuh"
 
 namespace tabi {
 void pack_atoms_dev(Handle& H, int nchr, const double* chrpos_dev, const double* atmchr_dev,
@@ -22,6 +26,11 @@ using namespace tabi;
 
 struct tabi_handle_s {
   Handle H;
+  WsNet* ws = nullptr;  // attached warm-start network (not owned)
+};
+
+struct tabi_ws_s {
+  WsNet* net = nullptr;
 };
 
 namespace {
@@ -153,6 +162,120 @@ template <typename T>
 void h2d(DBuf<T>& buf, const T* src, size_t n, cudaStream_t s) {
   buf.alloc(std::max<size_t>(n, 1));
   TABI_CUDA(cudaMemcpyAsync(buf.p, src, sizeof(T) * n, cudaMemcpyHostToDevice, s));
+}
+
+constexpr int kBatchStats = TABI_BATCH_STATS;
+
+struct MolDev {
+  int nspt;
+  const double* sptpos;
+  const double* sptnrm;
+  int nface;
+  const int* nvert;
+  int nchr;
+  const double* chrpos;
+  const double* atmchr;
+};
+
+template <typename M>
+void check_mol(const M& m) {
+  TABI_REQUIRE(m.nspt > 0 && m.nface > 0 && m.nchr > 0, TABI_ERR_ARG, "sizes must be positive");
+  TABI_REQUIRE(m.sptpos && m.sptnrm && m.nvert && m.chrpos && m.atmchr, TABI_ERR_ARG,
+               "null input");
+}
+
+// The whole main.f90 sequence for one molecule on device inputs: form_matrix,
+// tree, interaction lists, leaf LU, initial guess (zero, or the warm-start
+// network's prediction), solve, energy.  x_dev (tree order) may be null.
+void run_molecule(Handle& H, WsNet* ws, const MolDev& m, double* x_dev, double* stats,
+                  cudaStream_t s) {
+  check_mol(m);
+  const int nface = m.nface, nchr = m.nchr;
+  // TABI_TRACE=1 prints host wall time per phase (synchronising between them)
+  static const bool trace = getenv("TABI_TRACE") && getenv("TABI_TRACE")[0] == '1';
+  auto t_last = std::chrono::steady_clock::now();
+  auto mark = [&](const char* what) {
+    if (!trace) return;
+    cudaStreamSynchronize(s);
+    auto t = std::chrono::steady_clock::now();
+    fprintf(stderr, "[tabi] %-12s %9.3f ms\n", what,
+            std::chrono::duration<double, std::milli>(t - t_last).count());
+    t_last = t;
+  };
+  alloc_surface(H, nface);
+  pack_atoms_dev(H, nchr, m.chrpos, m.atmchr, s);
+  DBuf<double>& b0 = H.rn_b0;
+  DBuf<double>& b = H.rn_b;
+  b0.alloc(2 * (size_t)nface);
+  b.alloc(2 * (size_t)nface);
+  launch_form_matrix(H, m.nspt, m.sptpos, m.sptnrm, nface, m.nvert, nchr, H.d_atoms.p, b0.p, s);
+  H.has_surface = true;
+  mark("form_matrix");
+  build_tree(H, s);
+  mark("tree");
+  build_lists(H, s);
+  H.has_tree = true;
+  mark("lists");
+  build_precond(H, s);
+  mark("precond");
+  { TABI_K(K_FORM, s); permute_b_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(H.d_perm.p, nface, b0.p, b.p); }
+  DBuf<double>& xl = H.rn_x;
+  double* x = x_dev;
+  if (!x) {
+    xl.alloc(2 * (size_t)nface);
+    x = xl.p;
+  }
+  if (ws) {
+    // learned initial guess (tree order), GMRES from there
+    WsInput in;
+    in.n = nface;
+    in.px = H.d_x.p;
+    in.py = H.d_y.p;
+    in.pz = H.d_z.p;
+    in.qx = H.d_nx.p;
+    in.qy = H.d_ny.p;
+    in.qz = H.d_nz.p;
+    in.area = H.d_area.p;
+    in.b = b.p;
+    ws->forward(in, x, nullptr, s);
+    mark("warm start");
+  } else {
+    TABI_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * 2 * nface, s));
+  }
+  int iter = 0, ierr = 0;
+  double err = 0.0, se = 0.0, ce = 0.0;
+  solve_dev(H, b.p, x, &iter, &err, &ierr, nullptr, nullptr, s);
+  mark("gmres");
+  energy_dev(H, nchr, nullptr, nullptr, x, &se, &ce, s);
+  mark("energy");
+  if (stats) {
+    stats[0] = iter;
+    stats[1] = err;
+    stats[2] = ierr;
+    stats[3] = se;
+    stats[4] = ce;
+    stats[5] = (double)H.tree.n_near_pairs;
+    stats[6] = (double)H.tree.n_far;
+    stats[7] = H.tree.nleaf;
+  }
+}
+
+WsInput ws_input(int nface, const double* tr_xyz, const double* tr_q, const double* tr_area,
+                 const double* bvct) {
+  TABI_REQUIRE(nface > 0 && tr_xyz && tr_q && tr_area && bvct, TABI_ERR_ARG, "null argument");
+  WsInput in;
+  in.n = nface;
+  in.px = tr_xyz;
+  in.py = tr_xyz + 1;
+  in.pz = tr_xyz + 2;
+  in.ps = 3;
+  in.qx = tr_q;
+  in.qy = tr_q + 1;
+  in.qz = tr_q + 2;
+  in.qs = 3;
+  in.area = tr_area;
+  in.b = bvct;
+  return in;
 }
 
 }  // namespace
@@ -478,9 +601,6 @@ int tabi_run_dev(tabi_h h, int nspt, const double* sptpos_dev, const double* spt
   if (!h) return TABI_ERR_ARG;
   return guarded(h, [&] {
     Handle& H = h->H;
-    TABI_REQUIRE(nspt > 0 && nface > 0 && nchr > 0, TABI_ERR_ARG, "sizes must be positive");
-    TABI_REQUIRE(sptpos_dev && sptnrm_dev && nvert_dev && chrpos_dev && atmchr_dev,
-                 TABI_ERR_ARG, "null input");
     set_device(H);
     cudaStream_t s = pick(H, stream);
     cudaStream_t keep = H.stream;
@@ -490,58 +610,8 @@ int tabi_run_dev(tabi_h h, int nspt, const double* sptpos_dev, const double* spt
       cudaStream_t k;
       ~Restore() { H.stream = k; }
     } restore{H, keep};
-    // TABI_TRACE=1 prints host wall time per phase (synchronising between them)
-    static const bool trace = getenv("TABI_TRACE") && getenv("TABI_TRACE")[0] == '1';
-    auto t_last = std::chrono::steady_clock::now();
-    auto mark = [&](const char* what) {
-      if (!trace) return;
-      cudaStreamSynchronize(s);
-      auto t = std::chrono::steady_clock::now();
-      fprintf(stderr, "[tabi] %-12s %9.3f ms\n", what,
-              std::chrono::duration<double, std::milli>(t - t_last).count());
-      t_last = t;
-    };
-    alloc_surface(H, nface);
-    pack_atoms_dev(H, nchr, chrpos_dev, atmchr_dev, s);
-    DBuf<double>& b0 = H.rn_b0;
-    DBuf<double>& b = H.rn_b;
-    b0.alloc(2 * (size_t)nface);
-    b.alloc(2 * (size_t)nface);
-    launch_form_matrix(H, nspt, sptpos_dev, sptnrm_dev, nface, nvert_dev, nchr, H.d_atoms.p,
-                       b0.p, s);
-    H.has_surface = true;
-    mark("form_matrix");
-    build_tree(H, s);
-    mark("tree");
-    build_lists(H, s);
-    H.has_tree = true;
-    mark("lists");
-    build_precond(H, s);
-    mark("precond");
-    { TABI_K(K_FORM, s); permute_b_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(H.d_perm.p, nface, b0.p, b.p); }
-    DBuf<double>& xl = H.rn_x;
-    double* x = x_dev;
-    if (!x) {
-      xl.alloc(2 * (size_t)nface);
-      x = xl.p;
-    }
-    TABI_CUDA(cudaMemsetAsync(x, 0, sizeof(double) * 2 * nface, s));
-    int iter = 0, ierr = 0;
-    double err = 0.0, se = 0.0, ce = 0.0;
-    solve_dev(H, b.p, x, &iter, &err, &ierr, nullptr, nullptr, s);
-    mark("gmres");
-    energy_dev(H, nchr, nullptr, nullptr, x, &se, &ce, s);
-    mark("energy");
-    if (stats) {
-      stats[0] = iter;
-      stats[1] = err;
-      stats[2] = ierr;
-      stats[3] = se;
-      stats[4] = ce;
-      stats[5] = (double)H.tree.n_near_pairs;
-      stats[6] = (double)H.tree.n_far;
-      stats[7] = H.tree.nleaf;
-    }
+    MolDev m{nspt, sptpos_dev, sptnrm_dev, nface, nvert_dev, nchr, chrpos_dev, atmchr_dev};
+    run_molecule(H, h->ws, m, x_dev, stats, s);
   });
 }
 
@@ -654,6 +724,196 @@ int tabi_probe_fp64_peak(double ms, double* flops) {
     cudaEventDestroy(e1);
     double fl = 2.0 * 8 * 16 * (double)iters * blocks * threads;
     *flops = fl / (t * 1e-3);
+  });
+}
+
+// ---- learned warm start
+static cudaStream_t ws_stream(tabi_ws w, void* stream) {
+  return stream ? (cudaStream_t)stream : w->net->stream;
+}
+
+int tabi_ws_create(tabi_ws* w, int hidden, int layers, unsigned long long seed) {
+  if (!w) return TABI_ERR_ARG;
+  *w = nullptr;
+  return guarded(nullptr, [&] {
+    auto o = std::make_unique<tabi_ws_s>();
+    o->net = new WsNet(hidden, layers, seed);
+    *w = o.release();
+  });
+}
+
+int tabi_ws_destroy(tabi_ws w) {
+  if (!w) return TABI_ERR_ARG;
+  delete w->net;
+  delete w;
+  return TABI_OK;
+}
+
+long long tabi_ws_nparams(tabi_ws w) { return (w && w->net) ? (long long)w->net->np : -1; }
+
+int tabi_ws_get_params(tabi_ws w, float* theta, long long n) {
+  if (!w || !theta) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    TABI_REQUIRE(n == w->net->np, TABI_ERR_ARG, "parameter count mismatch");
+    w->net->get_params(theta);
+  });
+}
+
+int tabi_ws_set_params(tabi_ws w, const float* theta, long long n) {
+  if (!w || !theta) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    TABI_REQUIRE(n == w->net->np, TABI_ERR_ARG, "parameter count mismatch");
+    w->net->set_params(theta);
+  });
+}
+
+int tabi_ws_predict_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
+                        const double* tr_area, const double* bvct, double* x0, void* stream) {
+  if (!w) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    TABI_REQUIRE(x0 != nullptr, TABI_ERR_ARG, "null output");
+    cudaStream_t s = ws_stream(w, stream);
+    w->net->forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct), x0, nullptr, s);
+  });
+}
+
+int tabi_ws_loss_grad_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
+                          const double* tr_area, const double* bvct, const double* x_target,
+                          double* loss, float* grad, void* stream) {
+  if (!w) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    TABI_REQUIRE(x_target && loss, TABI_ERR_ARG, "null argument");
+    cudaStream_t s = ws_stream(w, stream);
+    WsNet& N = *w->net;
+    N.forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct), nullptr, x_target, s);
+    N.backward(nface, s);
+    *loss = N.read_loss(s);
+    if (grad) {
+      TABI_CUDA(cudaMemcpyAsync(grad, N.grad.p, sizeof(float) * N.np, cudaMemcpyDeviceToHost, s));
+      TABI_CUDA(cudaStreamSynchronize(s));
+    }
+  });
+}
+
+int tabi_ws_train_step_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
+                           const double* tr_area, const double* bvct, const double* x_target,
+                           double lr, double* loss, void* stream) {
+  if (!w) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    TABI_REQUIRE(x_target != nullptr, TABI_ERR_ARG, "null target");
+    TABI_REQUIRE(lr > 0.0 && std::isfinite(lr), TABI_ERR_ARG, "learning rate must be > 0");
+    cudaStream_t s = ws_stream(w, stream);
+    WsNet& N = *w->net;
+    N.forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct), nullptr, x_target, s);
+    N.backward(nface, s);
+    N.adam(lr, s);
+    if (loss) *loss = N.read_loss(s);
+  });
+}
+
+int tabi_ws_graph_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
+                      const double* tr_area, const double* bvct, int* nbr, float* feat,
+                      void* stream) {
+  if (!w) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    cudaStream_t s = ws_stream(w, stream);
+    WsNet& N = *w->net;
+    N.graph(ws_input(nface, tr_xyz, tr_q, tr_area, bvct), s);
+    TABI_REQUIRE(N.graph_exact(s), TABI_ERR_LIMIT,
+                 "neighbour search: the 16 nearest of some panel lie beyond 8 cells");
+    if (nbr)
+      TABI_CUDA(cudaMemcpyAsync(nbr, N.nbr.p, sizeof(int) * (size_t)nface * kWsK,
+                                cudaMemcpyDeviceToHost, s));
+    if (feat)
+      TABI_CUDA(cudaMemcpyAsync(feat, N.feat.p, sizeof(float) * (size_t)nface * kWsF,
+                                cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
+int tabi_set_warmstart(tabi_h h, tabi_ws w) {
+  if (!h) return TABI_ERR_ARG;
+  h->ws = w ? w->net : nullptr;
+  return TABI_OK;
+}
+
+// ---- batched solves
+int tabi_batch_run_dev(const tabi_params* p, int nmol, const tabi_mol_dev* mols, tabi_ws ws,
+                       int nworkers, double* stats) {
+  if (!p || !mols || nmol <= 0) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    check_params(*p);
+    TABI_REQUIRE(nworkers >= 1 && nworkers <= 64, TABI_ERR_ARG, "nworkers must be in 1..64");
+    for (int k = 0; k < nmol; ++k) {
+      check_mol(mols[k]);
+      TABI_REQUIRE(mols[k].maxparnode >= 0 && mols[k].order >= 0 && mols[k].order <= kMaxOrder,
+                   TABI_ERR_ARG, "per-molecule maxparnode / order out of range");
+    }
+    int dev = 0;
+    TABI_CUDA(cudaGetDevice(&dev));
+    // largest first (longest-processing-time order over the workers)
+    std::vector<int> order(nmol);
+    for (int k = 0; k < nmol; ++k) order[k] = k;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int a, int b) { return mols[a].nface > mols[b].nface; });
+    std::atomic<int> next{0};
+    std::atomic<bool> stop{false};
+    std::vector<std::string> errs(nworkers);
+    std::vector<int> codes(nworkers, TABI_OK);
+    const auto t0 = std::chrono::steady_clock::now();
+    auto ms_since = [&](std::chrono::steady_clock::time_point a,
+                        std::chrono::steady_clock::time_point b) {
+      return std::chrono::duration<double, std::milli>(b - a).count();
+    };
+    auto worker = [&](int w) {
+      tabi_h h = nullptr;
+      try {
+        TABI_CUDA(cudaSetDevice(dev));
+        int rc = tabi_create(&h, p);
+        TABI_REQUIRE(rc == TABI_OK, rc, "batch worker: cannot create a handle");
+        std::unique_ptr<WsNet> own;
+        if (ws) own = ws->net->clone();
+        for (;;) {
+          if (stop.load()) break;
+          const int k = next.fetch_add(1);
+          if (k >= nmol) break;
+          const tabi_mol_dev& md = mols[order[k]];
+          Handle& H = h->H;
+          H.prm = *p;
+          if (md.maxparnode > 0) H.prm.maxparnode = md.maxparnode;
+          if (md.order > 0) H.prm.order = md.order;
+          H.mv_prec = H.prm.precision;
+          double* st = stats ? stats + (size_t)kBatchStats * order[k] : nullptr;
+          const auto ta = std::chrono::steady_clock::now();
+          MolDev m{md.nspt, md.sptpos, md.sptnrm, md.nface, md.nvert, md.nchr, md.chrpos,
+                   md.atmchr};
+          run_molecule(H, own.get(), m, nullptr, st, H.stream);
+          TABI_CUDA(cudaStreamSynchronize(H.stream));
+          const auto tb = std::chrono::steady_clock::now();
+          if (st) {
+            st[8] = ms_since(ta, tb);
+            st[9] = ms_since(t0, tb);
+            st[10] = w;
+            st[11] = H.prm.maxparnode;
+          }
+        }
+      } catch (const Error& e) {
+        errs[w] = e.what();
+        codes[w] = e.code;
+        stop = true;
+      } catch (const std::exception& e) {
+        errs[w] = e.what();
+        codes[w] = TABI_ERR_CUDA;
+        stop = true;
+      }
+      if (h) tabi_destroy(h);
+    };
+    std::vector<std::thread> th;
+    for (int w = 0; w < nworkers; ++w) th.emplace_back(worker, w);
+    for (auto& t : th) t.join();
+    for (int w = 0; w < nworkers; ++w)
+      TABI_REQUIRE(codes[w] == TABI_OK, codes[w],
+                   "batch worker " + std::to_string(w) + ": " + errs[w]);
   });
 }
 

@@ -1,0 +1,1012 @@
+// warmstart.cu -- the learned warm start: a rotation- and translation-invariant
+// point-cloud network over surface panels that predicts the initial surface
+// potential and normal derivative x0 = [phi; dphi/dn] of a solve from the
+// panel geometry and the right-hand side (main.f90:592-606).  It has no
+// counterpart in the reference, which always starts GMRES from zero
+// (main.f90:133); GMRES on the true residual stays the judge, so a prediction
+// only changes the iteration count.
+//
+// Network, for N panels (centroid r, unit normal n, area A, b = [b1; b2]):
+//   graph   K = 16 nearest other panels per panel (cell-list search, exact,
+//           ascending distance, ties by index)
+//   input   8 invariant node features and 11 invariant edge features (8
+//           radial basis functions of |r_ij| / mean neighbour distance and
+//           three normal/direction cosines)
+//   layers  h = silu(f W0 + b0); L times: u = h Wa,
+//           a_i = 1/K sum_k silu(e_ij Wf + bf) * u_j, z = h Wb1 + a Wb2 + bb,
+//           h += silu(z)
+//   output  o = h Wo + bo, x1 = s o0, x2 = b2 + s o1 with s = rms(b1)
+// Weight matrices are used in bfloat16 with FP32 accumulation; FP32 master
+// weights, gradients and Adam moments are kept for training.  Every reduction
+// (weight gradients, bias gradients, loss) is a fixed-order two-stage sum, and
+// the scatter of the aggregation's backward pass runs as a gather over the
+// reversed neighbour lists, so a training step is deterministic.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <random>
+
+#include "tabi_impl.cuh"
+#include "warmstart.cuh"
+
+namespace tabi {
+
+namespace {
+
+constexpr int kK = kWsK;      // neighbours
+constexpr int kR = kWsR;      // radial basis functions
+constexpr int kE = kWsR + 3;  // edge features
+constexpr int kF = kWsF;      // node features
+constexpr int kRedB = 592;    // blocks of the fixed-grid reductions
+constexpr int kWsBlocks = 592;
+
+__device__ __forceinline__ float sigm(float x) { return 1.f / (1.f + __expf(-x)); }
+__device__ __forceinline__ float silu(float x) { return x * sigm(x); }
+__device__ __forceinline__ float dsilu(float x) {
+  const float s = sigm(x);
+  return s * (1.f + x * (1.f - s));
+}
+
+// ---------------------------------------------------------------- inputs
+// Panels to FP32 (position + area, normal) from strided FP64 components, and
+// per-block partial sums of area, b1^2 and the bounding box.
+__global__ void ws_prep_kernel(int n, const double* __restrict__ px, const double* __restrict__ py,
+                               const double* __restrict__ pz, int ps,
+                               const double* __restrict__ qx, const double* __restrict__ qy,
+                               const double* __restrict__ qz, int qs,
+                               const double* __restrict__ area, const double* __restrict__ b,
+                               float4* __restrict__ pos, float4* __restrict__ nrm,
+                               float2* __restrict__ bf, double* __restrict__ part) {
+  double sa = 0.0, sb = 0.0;
+  float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    const double x = px[(size_t)i * ps], y = py[(size_t)i * ps], z = pz[(size_t)i * ps];
+    const double a = area[i];
+    pos[i] = make_float4((float)x, (float)y, (float)z, (float)a);
+    nrm[i] = make_float4((float)qx[(size_t)i * qs], (float)qy[(size_t)i * qs],
+                         (float)qz[(size_t)i * qs], 0.f);
+    bf[i] = make_float2((float)b[i], (float)b[n + i]);
+    sa += a;
+    sb += b[i] * b[i];
+    const float c[3] = {(float)x, (float)y, (float)z};
+    for (int d = 0; d < 3; ++d) {
+      lo[d] = fminf(lo[d], c[d]);
+      hi[d] = fmaxf(hi[d], c[d]);
+    }
+  }
+  __shared__ double s[8][256];
+  const int t = threadIdx.x;
+  s[0][t] = sa;
+  s[1][t] = sb;
+  for (int d = 0; d < 3; ++d) {
+    s[2 + d][t] = lo[d];
+    s[5 + d][t] = hi[d];
+  }
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if (t < w) {
+      s[0][t] += s[0][t + w];
+      s[1][t] += s[1][t + w];
+      for (int d = 0; d < 3; ++d) {
+        s[2 + d][t] = fmin(s[2 + d][t], s[2 + d][t + w]);
+        s[5 + d][t] = fmax(s[5 + d][t], s[5 + d][t + w]);
+      }
+    }
+    __syncthreads();
+  }
+  if (t < 8) part[blockIdx.x * 8 + t] = s[t][0];
+}
+
+__global__ void ws_prep_final_kernel(const double* __restrict__ part, int nb, double* out) {
+  if (threadIdx.x != 0) return;
+  double v[8] = {0, 0, 3e38, 3e38, 3e38, -3e38, -3e38, -3e38};
+  for (int k = 0; k < nb; ++k) {
+    v[0] += part[8 * k];
+    v[1] += part[8 * k + 1];
+    for (int d = 0; d < 3; ++d) {
+      v[2 + d] = fmin(v[2 + d], part[8 * k + 2 + d]);
+      v[5 + d] = fmax(v[5 + d], part[8 * k + 5 + d]);
+    }
+  }
+  for (int k = 0; k < 8; ++k) out[k] = v[k];
+}
+
+// ---------------------------------------------------------------- graph
+struct Grid {
+  float x0, y0, z0, h;
+  int nx, ny, nz;
+};
+
+__device__ __forceinline__ int cell_coord(float v, float v0, float h, int nmax) {
+  int c = (int)floorf((v - v0) / h);
+  return min(max(c, 0), nmax - 1);
+}
+
+__global__ void ws_cell_count_kernel(int n, const float4* __restrict__ pos, Grid g,
+                                     int* __restrict__ cell, int* __restrict__ cnt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  float4 p = pos[i];
+  int c = (cell_coord(p.z, g.z0, g.h, g.nz) * g.ny + cell_coord(p.y, g.y0, g.h, g.ny)) * g.nx +
+          cell_coord(p.x, g.x0, g.h, g.nx);
+  cell[i] = c;
+  atomicAdd(&cnt[c], 1);
+}
+
+__global__ void ws_cell_fill_kernel(int n, const int* __restrict__ cell,
+                                    int* __restrict__ cursor, int* __restrict__ sorted) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  sorted[atomicAdd(&cursor[cell[i]], 1)] = i;
+}
+
+// exclusive scan of cnt[0..m) into off[0..m], three passes (block sums,
+// scan of the block sums, add)
+constexpr int kScanB = 1024;
+__global__ void ws_scan_block_kernel(const int* __restrict__ in, int m, int* __restrict__ out,
+                                     int* __restrict__ bsum) {
+  __shared__ int s[kScanB];
+  int i = blockIdx.x * kScanB + threadIdx.x;
+  int v = i < m ? in[i] : 0;
+  s[threadIdx.x] = v;
+  __syncthreads();
+  for (int o = 1; o < kScanB; o <<= 1) {
+    int t = threadIdx.x >= o ? s[threadIdx.x - o] : 0;
+    __syncthreads();
+    s[threadIdx.x] += t;
+    __syncthreads();
+  }
+  if (i < m) out[i] = s[threadIdx.x] - v;
+  if (threadIdx.x == kScanB - 1) bsum[blockIdx.x] = s[threadIdx.x];
+}
+
+__global__ void ws_scan_sums_kernel(int* __restrict__ bsum, int nb, int* __restrict__ total) {
+  if (threadIdx.x != 0) return;
+  int acc = 0;
+  for (int k = 0; k < nb; ++k) {
+    int v = bsum[k];
+    bsum[k] = acc;
+    acc += v;
+  }
+  *total = acc;
+}
+
+__global__ void ws_scan_add_kernel(int* __restrict__ out, int m, const int* __restrict__ bsum,
+                                   const int* __restrict__ total) {
+  int i = blockIdx.x * kScanB + threadIdx.x;
+  if (i < m) out[i] += bsum[blockIdx.x];
+  if (i == 0) out[m] = *total;
+}
+
+// K nearest other panels: search the cube of cells within +-rad of the
+// panel's cell; the result is exact once the K-th distance is within rad*h
+// (the cube contains that ball), else the cube grows (to rad = 8).
+__global__ void ws_knn_kernel(int n, const float4* __restrict__ pos, Grid g,
+                              const int* __restrict__ coff, const int* __restrict__ sorted,
+                              int* __restrict__ nbr, int* __restrict__ err) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p = pos[i];
+  const int cx = cell_coord(p.x, g.x0, g.h, g.nx), cy = cell_coord(p.y, g.y0, g.h, g.ny),
+            cz = cell_coord(p.z, g.z0, g.h, g.nz);
+  float bd[kK];
+  int bi[kK];
+  for (int rad = 1;; ++rad) {
+#pragma unroll
+    for (int k = 0; k < kK; ++k) {
+      bd[k] = 3e38f;
+      bi[k] = 0x7fffffff;
+    }
+    for (int z = max(cz - rad, 0); z <= min(cz + rad, g.nz - 1); ++z)
+      for (int y = max(cy - rad, 0); y <= min(cy + rad, g.ny - 1); ++y)
+        for (int x = max(cx - rad, 0); x <= min(cx + rad, g.nx - 1); ++x) {
+          const int c = (z * g.ny + y) * g.nx + x;
+          for (int q = coff[c]; q < coff[c + 1]; ++q) {
+            const int j = sorted[q];
+            if (j == i) continue;
+            const float4 o = pos[j];
+            const float dx = o.x - p.x, dy = o.y - p.y, dz = o.z - p.z;
+            const float d = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+            if (d > bd[kK - 1] || (d == bd[kK - 1] && j > bi[kK - 1])) continue;
+            // insert (d, j) keeping (distance, index) ascending
+            float cd = d;
+            int cj = j;
+#pragma unroll
+            for (int k = 0; k < kK; ++k) {
+              const bool less = cd < bd[k] || (cd == bd[k] && cj < bi[k]);
+              const float td = bd[k];
+              const int tj = bi[k];
+              bd[k] = less ? cd : td;
+              bi[k] = less ? cj : tj;
+              cd = less ? td : cd;
+              cj = less ? tj : cj;
+            }
+          }
+        }
+    const float reach = rad * g.h;
+    const bool whole = cx - rad <= 0 && cy - rad <= 0 && cz - rad <= 0 && cx + rad >= g.nx - 1 &&
+                       cy + rad >= g.ny - 1 && cz + rad >= g.nz - 1;
+    if ((bi[kK - 1] != 0x7fffffff && bd[kK - 1] <= reach * reach) || whole) break;
+    if (rad == 8) {
+      atomicExch(err, 1);  // not exact: the K nearest lie beyond 8 cells
+      break;
+    }
+  }
+#pragma unroll
+  for (int k = 0; k < kK; ++k) nbr[(size_t)i * kK + k] = bi[k] == 0x7fffffff ? i : bi[k];
+}
+
+// reversed neighbour lists: for panel j, the edges (i, k) with nbr(i, k) = j
+__global__ void ws_rev_count_kernel(int n, const int* __restrict__ nbr, int* __restrict__ cnt) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * kK) return;
+  atomicAdd(&cnt[nbr[e]], 1);
+}
+
+__global__ void ws_rev_fill_kernel(int n, const int* __restrict__ nbr, int* __restrict__ cursor,
+                                   int* __restrict__ rev) {
+  int e = blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= n * kK) return;
+  rev[atomicAdd(&cursor[nbr[e]], 1)] = e;
+}
+
+// each list in ascending edge id (fixed order for the gather)
+__global__ void ws_rev_sort_kernel(int n, const int* __restrict__ off, int* __restrict__ rev) {
+  int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= n) return;
+  const int a = off[j], b = off[j + 1];
+  for (int p = a + 1; p < b; ++p) {
+    int v = rev[p], q = p - 1;
+    while (q >= a && rev[q] > v) {
+      rev[q + 1] = rev[q];
+      --q;
+    }
+    rev[q + 1] = v;
+  }
+}
+
+// edge features e_ij (kE) of panel i's neighbour j
+__device__ __forceinline__ void edge_feat(const float4 pi, const float4 ni, const float4 pj,
+                                          const float4 nj, float dbar, float* e) {
+  const float rx = pj.x - pi.x, ry = pj.y - pi.y, rz = pj.z - pi.z;
+  const float d = sqrtf(fmaf(rx, rx, fmaf(ry, ry, rz * rz)));
+  const float inv = d > 0.f ? 1.f / d : 0.f;
+  const float rho = d / dbar;
+  const float sig = 2.5f / (kR - 1);
+#pragma unroll
+  for (int m = 0; m < kR; ++m) {
+    const float t = (rho - sig * m) / sig;
+    e[m] = __expf(-t * t);
+  }
+  e[kR] = fmaf(ni.x, nj.x, fmaf(ni.y, nj.y, ni.z * nj.z));
+  e[kR + 1] = fmaf(ni.x, rx, fmaf(ni.y, ry, ni.z * rz)) * inv;
+  e[kR + 2] = fmaf(nj.x, rx, fmaf(nj.y, ry, nj.z * rz)) * inv;
+}
+
+// node features (kF per panel) and the mean neighbour distance
+__global__ void ws_node_kernel(int n, const float4* __restrict__ pos, const float4* __restrict__ nrm,
+                               const float2* __restrict__ bf, const int* __restrict__ nbr,
+                               const double* __restrict__ stats, float* __restrict__ dbar_out,
+                               float* __restrict__ f) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float abar = (float)(stats[0] / n);
+  double ms = stats[1] / n;
+  const float s = ms > 0.0 ? (float)sqrt(ms) : 1.f;
+  const float4 p = pos[i], q = nrm[i];
+  const float2 bi = bf[i];
+  float dsum = 0.f, curv = 0.f, nn = 0.f, db = 0.f;
+  float dd[kK], hh[kK];
+#pragma unroll
+  for (int k = 0; k < kK; ++k) {
+    const int j = nbr[(size_t)i * kK + k];
+    const float4 o = pos[j], m = nrm[j];
+    const float rx = o.x - p.x, ry = o.y - p.y, rz = o.z - p.z;
+    const float d2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+    dd[k] = d2;
+    hh[k] = fmaf(q.x, rx, fmaf(q.y, ry, q.z * rz));
+    dsum += sqrtf(d2);
+    nn += fmaf(q.x, m.x, fmaf(q.y, m.y, q.z * m.z));
+    db += (bf[j].x - bi.x) / s;
+  }
+  const float dbar = fmaxf(dsum / kK, 1e-6f);
+#pragma unroll
+  for (int k = 0; k < kK; ++k) curv += dd[k] > 0.f ? hh[k] * dbar / dd[k] : 0.f;
+  dbar_out[i] = dbar;
+  float* o = f + (size_t)i * kF;
+  o[0] = bi.x / s;
+  o[1] = bi.y / s;
+  o[2] = logf(fmaxf(p.w / abar, 1e-6f));
+  o[3] = logf(abar);
+  o[4] = curv / kK;
+  o[5] = nn / kK;
+  o[6] = logf(dbar);
+  o[7] = db / kK;
+}
+
+// ---------------------------------------------------------------- dense layers
+// C (M x N) = A (M x Kd, FP32, row-major) * B, B in bfloat16: B(k, c) = W[k*ldw + c]
+// (TB = false) or W[c*ldw + k] (TB = true, i.e. A * W^T).  64 x 64 tiles,
+// 16-deep k steps, 4 x 4 outputs per thread.  Epilogues:
+//   0: C = acc            1: C = acc + bias          2: C += acc
+//   3: P = acc + bias, C = silu(P)
+//   4: P = P_in + acc, C = R + silu(P)  (second half of z = h Wb1 + a Wb2 + bb,
+//      P_in = h Wb1 + bb; R the residual input h)
+constexpr int kGM = 64, kGN = 64, kGK = 16;
+
+template <bool TB, int EPI>
+__global__ void __launch_bounds__(256) ws_gemm_kernel(int M, int N, int Kd,
+                                                      const float* __restrict__ A, int lda,
+                                                      const __nv_bfloat16* __restrict__ W,
+                                                      int ldw, const float* __restrict__ bias,
+                                                      float* __restrict__ C, int ldc,
+                                                      float* __restrict__ P,
+                                                      const float* __restrict__ Rin) {
+  __shared__ float As[kGK][kGM + 4];
+  __shared__ float Bs[kGK][kGN + 4];
+  const int tid = threadIdx.x;
+  const int tr = tid / 16, tc = tid % 16;
+  const int row0 = blockIdx.x * kGM, col0 = blockIdx.y * kGN;
+  float acc[4][4] = {};
+  for (int k0 = 0; k0 < Kd; k0 += kGK) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + q * 256;  // 0..1023
+      const int r = e / kGK, k = e % kGK;
+      const int gr = row0 + r, gk = k0 + k;
+      As[k][r] = (gr < M && gk < Kd) ? A[(size_t)gr * lda + gk] : 0.f;
+      const int bk = e / kGN, bc = e % kGN;
+      const int gbk = k0 + bk, gbc = col0 + bc;
+      float w = 0.f;
+      if (gbk < Kd && gbc < N)
+        w = __bfloat162float(TB ? W[(size_t)gbc * ldw + gbk] : W[(size_t)gbk * ldw + gbc]);
+      Bs[bk][bc] = w;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < kGK; ++k) {
+      float a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[k][tr * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[k][tc * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = row0 + tr * 4 + i;
+    if (r >= M) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = col0 + tc * 4 + j;
+      if (c >= N) continue;
+      const size_t o = (size_t)r * ldc + c;
+      const float v = acc[i][j];
+      if (EPI == 0) C[o] = v;
+      if (EPI == 1) C[o] = v + bias[c];
+      if (EPI == 2) C[o] += v;
+      if (EPI == 3) {
+        const float pr = v + bias[c];
+        P[o] = pr;
+        C[o] = silu(pr);
+      }
+      if (EPI == 4) {
+        const float pr = P[o] + v;
+        P[o] = pr;
+        C[o] = Rin[o] + silu(pr);
+      }
+    }
+  }
+}
+
+// Weight gradient partials: part[chunk] (Kd x N) = A[rows of chunk]^T * D[rows of chunk]
+constexpr int kDWChunk = 4096;
+__global__ void __launch_bounds__(256) ws_dw_kernel(int M, int Kd, int N,
+                                                    const float* __restrict__ A, int lda,
+                                                    const float* __restrict__ D, int ldd,
+                                                    float* __restrict__ part) {
+  __shared__ float As[kGK][kGM + 4];
+  __shared__ float Ds[kGK][kGN + 4];
+  const int tid = threadIdx.x;
+  const int tr = tid / 16, tc = tid % 16;
+  const int k0 = blockIdx.x * kGM, c0 = blockIdx.y * kGN;
+  const int m0 = blockIdx.z * kDWChunk, m1 = min(M, m0 + kDWChunk);
+  float acc[4][4] = {};
+  for (int mb = m0; mb < m1; mb += kGK) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int e = tid + q * 256;
+      const int r = e / kGM, c = e % kGM;  // r: row within the 16-row step
+      const int gm = mb + r;
+      As[r][c] = (gm < m1 && k0 + c < Kd) ? A[(size_t)gm * lda + k0 + c] : 0.f;
+      Ds[r][c] = (gm < m1 && c0 + c < N) ? D[(size_t)gm * ldd + c0 + c] : 0.f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kGK; ++r) {
+      float a[4], d[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[r][tr * 4 + i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) d[j] = Ds[r][tc * 4 + j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], d[j], acc[i][j]);
+    }
+    __syncthreads();
+  }
+  float* out = part + (size_t)blockIdx.z * Kd * N;
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int k = k0 + tr * 4 + i;
+    if (k >= Kd) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = c0 + tc * 4 + j;
+      if (c < N) out[(size_t)k * N + c] = acc[i][j];
+    }
+  }
+}
+
+// g[e] = sum over chunks of part[chunk][e], in chunk order
+__global__ void ws_sum_parts_kernel(const float* __restrict__ part, int nchunk, int64_t len,
+                                    float* __restrict__ g) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < len;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    float s = 0.f;
+    for (int c = 0; c < nchunk; ++c) s += part[(size_t)c * len + e];
+    g[e] = s;
+  }
+}
+
+// column sums of X (M x N) into part[block][N] (fixed row ranges per block)
+__global__ void ws_colsum_kernel(int M, int N, const float* __restrict__ X,
+                                 float* __restrict__ part) {
+  const int per = (M + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * per, r1 = min(M, r0 + per);
+  for (int c = threadIdx.x; c < N; c += blockDim.x) {
+    float s = 0.f;
+    for (int r = r0; r < r1; ++r) s += X[(size_t)r * N + c];
+    part[(size_t)blockIdx.x * N + c] = s;
+  }
+}
+
+// elementwise: out = g * silu'(x)
+__global__ void ws_dsilu_kernel(int64_t len, const float* __restrict__ g,
+                                const float* __restrict__ x, float* __restrict__ out) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < len;
+       e += (int64_t)gridDim.x * blockDim.x)
+    out[e] = g[e] * dsilu(x[e]);
+}
+
+// ---------------------------------------------------------------- aggregation
+// a_i = 1/K sum_k silu(e_ik Wf + bf) * u_{nbr(i,k)}; one thread per channel,
+// kWsNodes panels per block.
+constexpr int kWsNodes = 8;
+
+__global__ void ws_agg_fwd_kernel(int n, int H, const float4* __restrict__ pos,
+                                  const float4* __restrict__ nrm, const float* __restrict__ dbar,
+                                  const int* __restrict__ nbr,
+                                  const __nv_bfloat16* __restrict__ Wf,
+                                  const float* __restrict__ bfv, const float* __restrict__ u,
+                                  float* __restrict__ a) {
+  __shared__ float es[kK][kE];
+  __shared__ int js[kK];
+  const int c = threadIdx.x;
+  float w[kE];
+#pragma unroll
+  for (int q = 0; q < kE; ++q) w[q] = __bfloat162float(Wf[(size_t)q * H + c]);
+  const float bc = bfv[c];
+  for (int t = 0; t < kWsNodes; ++t) {
+    const int i = blockIdx.x * kWsNodes + t;
+    if (i >= n) break;
+    __syncthreads();
+    if (c < kK) {
+      const int j = nbr[(size_t)i * kK + c];
+      js[c] = j;
+      float e[kE];
+      edge_feat(pos[i], nrm[i], pos[j], nrm[j], dbar[i], e);
+#pragma unroll
+      for (int q = 0; q < kE; ++q) es[c][q] = e[q];
+    }
+    __syncthreads();
+    float acc = 0.f;
+#pragma unroll 4
+    for (int k = 0; k < kK; ++k) {
+      float pr = bc;
+#pragma unroll
+      for (int q = 0; q < kE; ++q) pr = fmaf(es[k][q], w[q], pr);
+      acc = fmaf(silu(pr), u[(size_t)js[k] * H + c], acc);
+    }
+    a[(size_t)i * H + c] = acc * (1.f / kK);
+  }
+}
+
+// Backward of the aggregation, part 1 (per panel i, contiguous panel ranges
+// per block): dpre_ik = u_j da_i / K * silu'(pre_ik); per-block partial
+// gradients of Wf (kE x H) and bf (H).
+__global__ void ws_agg_bwd_w_kernel(int n, int H, const float4* __restrict__ pos,
+                                    const float4* __restrict__ nrm,
+                                    const float* __restrict__ dbar, const int* __restrict__ nbr,
+                                    const __nv_bfloat16* __restrict__ Wf,
+                                    const float* __restrict__ bfv, const float* __restrict__ u,
+                                    const float* __restrict__ da, float* __restrict__ part) {
+  __shared__ float es[kK][kE];
+  __shared__ int js[kK];
+  const int c = threadIdx.x;
+  float w[kE], gw[kE];
+#pragma unroll
+  for (int q = 0; q < kE; ++q) {
+    w[q] = __bfloat162float(Wf[(size_t)q * H + c]);
+    gw[q] = 0.f;
+  }
+  float gb = 0.f;
+  const float bc = bfv[c];
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+  for (int i = i0; i < i1; ++i) {
+    __syncthreads();
+    if (c < kK) {
+      const int j = nbr[(size_t)i * kK + c];
+      js[c] = j;
+      float e[kE];
+      edge_feat(pos[i], nrm[i], pos[j], nrm[j], dbar[i], e);
+#pragma unroll
+      for (int q = 0; q < kE; ++q) es[c][q] = e[q];
+    }
+    __syncthreads();
+    const float g = da[(size_t)i * H + c] * (1.f / kK);
+    for (int k = 0; k < kK; ++k) {
+      float pr = bc;
+#pragma unroll
+      for (int q = 0; q < kE; ++q) pr = fmaf(es[k][q], w[q], pr);
+      const float dp = u[(size_t)js[k] * H + c] * g * dsilu(pr);
+#pragma unroll
+      for (int q = 0; q < kE; ++q) gw[q] = fmaf(es[k][q], dp, gw[q]);
+      gb += dp;
+    }
+  }
+  float* o = part + (size_t)blockIdx.x * (kE + 1) * H;
+#pragma unroll
+  for (int q = 0; q < kE; ++q) o[(size_t)q * H + c] = gw[q];
+  o[(size_t)kE * H + c] = gb;
+}
+
+// Backward of the aggregation, part 2 (per panel j, over the reversed lists):
+// du_j = sum_{(i,k): nbr(i,k) = j} silu(pre_ik) da_i / K
+__global__ void ws_agg_bwd_u_kernel(int n, int H, const float4* __restrict__ pos,
+                                    const float4* __restrict__ nrm,
+                                    const float* __restrict__ dbar, const int* __restrict__ roff,
+                                    const int* __restrict__ rev,
+                                    const __nv_bfloat16* __restrict__ Wf,
+                                    const float* __restrict__ bfv, const float* __restrict__ da,
+                                    float* __restrict__ du) {
+  __shared__ float es[32][kE];
+  __shared__ int is[32];
+  const int c = threadIdx.x;
+  float w[kE];
+#pragma unroll
+  for (int q = 0; q < kE; ++q) w[q] = __bfloat162float(Wf[(size_t)q * H + c]);
+  const float bc = bfv[c];
+  for (int t = 0; t < kWsNodes; ++t) {
+    const int j = blockIdx.x * kWsNodes + t;
+    if (j >= n) break;
+    const int a0 = roff[j], a1 = roff[j + 1];
+    float acc = 0.f;
+    for (int b0 = a0; b0 < a1; b0 += 32) {
+      const int cnt = min(32, a1 - b0);
+      __syncthreads();
+      if (c < cnt) {
+        const int i = rev[b0 + c] / kK;
+        is[c] = i;
+        float e[kE];
+        edge_feat(pos[i], nrm[i], pos[j], nrm[j], dbar[i], e);
+#pragma unroll
+        for (int q = 0; q < kE; ++q) es[c][q] = e[q];
+      }
+      __syncthreads();
+      for (int k = 0; k < cnt; ++k) {
+        float pr = bc;
+#pragma unroll
+        for (int q = 0; q < kE; ++q) pr = fmaf(es[k][q], w[q], pr);
+        acc = fmaf(silu(pr), da[(size_t)is[k] * H + c], acc);
+      }
+    }
+    du[(size_t)j * H + c] = acc * (1.f / kK);
+  }
+}
+
+// ---------------------------------------------------------------- head / loss
+// o = h Wo + bo (one warp per panel); x = [s o0, b2 + s o1]; with a target,
+// do = 2 (o - t) / N and per-block loss partials.
+__global__ void ws_head_kernel(int n, int H, const float* __restrict__ h,
+                               const __nv_bfloat16* __restrict__ Wo,
+                               const float* __restrict__ bo, const double* __restrict__ b,
+                               const double* __restrict__ stats, double* __restrict__ xout,
+                               const double* __restrict__ target, float* __restrict__ dout,
+                               double* __restrict__ lpart) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double ms = stats[1] / n;
+  const double s = ms > 0.0 ? sqrt(ms) : 1.0;
+  double lsum = 0.0;
+  const int per = (n + gridDim.x - 1) / gridDim.x;
+  const int i0 = blockIdx.x * per, i1 = min(n, i0 + per);
+  for (int i = i0 + warp; i < i1; i += blockDim.x / 32) {
+    float o0 = 0.f, o1 = 0.f;
+    for (int c = lane; c < H; c += 32) {
+      const float v = h[(size_t)i * H + c];
+      o0 = fmaf(v, __bfloat162float(Wo[2 * c]), o0);
+      o1 = fmaf(v, __bfloat162float(Wo[2 * c + 1]), o1);
+    }
+    for (int off = 16; off > 0; off >>= 1) {
+      o0 += __shfl_xor_sync(0xffffffffu, o0, off);
+      o1 += __shfl_xor_sync(0xffffffffu, o1, off);
+    }
+    o0 += bo[0];
+    o1 += bo[1];
+    if (lane == 0) {
+      if (xout) {
+        xout[i] = s * o0;
+        xout[n + i] = b[n + i] + s * o1;
+      }
+      if (target) {
+        const double t0 = target[i] / s, t1 = (target[n + i] - b[n + i]) / s;
+        const double d0 = o0 - t0, d1 = o1 - t1;
+        lsum += d0 * d0 + d1 * d1;
+        dout[2 * i] = (float)(2.0 * d0 / n);
+        dout[2 * i + 1] = (float)(2.0 * d1 / n);
+      }
+    }
+  }
+  if (!target) return;
+  __shared__ double sl[32];
+  if (lane == 0) sl[warp] = lsum;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double t = 0.0;
+    for (int w = 0; w < (int)blockDim.x / 32; ++w) t += sl[w];
+    lpart[blockIdx.x] = t;
+  }
+}
+
+__global__ void ws_loss_final_kernel(const double* __restrict__ lpart, int nb, int n,
+                                     double* __restrict__ out) {
+  if (threadIdx.x != 0) return;
+  double t = 0.0;
+  for (int k = 0; k < nb; ++k) t += lpart[k];
+  out[0] = t / n;
+}
+
+// dh = do Wo^T (N x H)
+__global__ void ws_head_bwd_kernel(int n, int H, const float* __restrict__ dout,
+                                   const __nv_bfloat16* __restrict__ Wo, float* __restrict__ dh) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < (int64_t)n * H;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int i = (int)(e / H), c = (int)(e % H);
+    dh[e] = dout[2 * i] * __bfloat162float(Wo[2 * c]) +
+            dout[2 * i + 1] * __bfloat162float(Wo[2 * c + 1]);
+  }
+}
+
+// ---------------------------------------------------------------- optimiser
+__global__ void ws_adam_kernel(int64_t np, float* __restrict__ theta, const float* __restrict__ g,
+                               float* __restrict__ m, float* __restrict__ v, float lr, float b1,
+                               float b2, float c1, float c2, float eps,
+                               __nv_bfloat16* __restrict__ wbf) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < np;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const float gv = g[e];
+    const float mv = b1 * m[e] + (1.f - b1) * gv;
+    const float vv = b2 * v[e] + (1.f - b2) * gv * gv;
+    m[e] = mv;
+    v[e] = vv;
+    const float t = theta[e] - lr * (mv / c1) / (sqrtf(vv / c2) + eps);
+    theta[e] = t;
+    wbf[e] = __float2bfloat16_rn(t);
+  }
+}
+
+__global__ void ws_to_bf16_kernel(int64_t np, const float* __restrict__ theta,
+                                  __nv_bfloat16* __restrict__ wbf) {
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < np;
+       e += (int64_t)gridDim.x * blockDim.x)
+    wbf[e] = __float2bfloat16_rn(theta[e]);
+}
+
+template <bool TB, int EPI>
+void gemm(int M, int N, int Kd, const float* A, int lda, const __nv_bfloat16* W, int ldw,
+          const float* bias, float* C, int ldc, float* P, const float* R, cudaStream_t s) {
+  dim3 grid(ceil_div(M, kGM), ceil_div(N, kGN));
+  ws_gemm_kernel<TB, EPI><<<grid, 256, 0, s>>>(M, N, Kd, A, lda, W, ldw, bias, C, ldc, P, R);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- host side
+WsNet::WsNet(int hidden, int layers, unsigned long long seed) : H(hidden), L(layers) {
+  TABI_REQUIRE(H >= 32 && H <= 256 && H % 32 == 0, TABI_ERR_ARG,
+               "hidden width must be a multiple of 32 in 32..256");
+  TABI_REQUIRE(L >= 1 && L <= 8, TABI_ERR_ARG, "layers must be in 1..8");
+  // flat layout: W0 b0 | per layer Wa Wf bf Wb1 Wb2 bb | Wo bo
+  int64_t o = 0;
+  auto take = [&](int64_t k) {
+    int64_t r = o;
+    o += k;
+    return r;
+  };
+  off_W0 = take((int64_t)kF * H);
+  off_b0 = take(H);
+  for (int l = 0; l < L; ++l) {
+    Layer y;
+    y.Wa = take((int64_t)H * H);
+    y.Wf = take((int64_t)kE * H);
+    y.bf = take(H);
+    y.Wb1 = take((int64_t)H * H);
+    y.Wb2 = take((int64_t)H * H);
+    y.bb = take(H);
+    lay.push_back(y);
+  }
+  off_Wo = take((int64_t)H * 2);
+  off_bo = take(2);
+  np = o;
+  // initial weights: N(0, 1/fan_in) for the matrices (the output layer zero,
+  // so an untrained network predicts x1 = 0, x2 = b2), zero biases
+  std::vector<float> th((size_t)np, 0.f);
+  std::mt19937_64 rng(seed);
+  std::normal_distribution<double> nd(0.0, 1.0);
+  auto fill = [&](int64_t at, int rows, int cols, double scale) {
+    for (int64_t k = 0; k < (int64_t)rows * cols; ++k) th[at + k] = (float)(nd(rng) * scale);
+  };
+  fill(off_W0, kF, H, 1.0 / std::sqrt((double)kF));
+  for (auto& y : lay) {
+    fill(y.Wa, H, H, 1.0 / std::sqrt((double)H));
+    fill(y.Wf, kE, H, 1.0 / std::sqrt((double)kE));
+    fill(y.Wb1, H, H, 0.5 / std::sqrt((double)H));
+    fill(y.Wb2, H, H, 0.5 / std::sqrt((double)H));
+  }
+  TABI_CUDA(cudaStreamCreateWithFlags(&stream, cudaStreamNonBlocking));
+  TABI_CUDA(cudaMallocHost(&h_stats, sizeof(double) * 16));
+  theta.alloc(np);
+  wbf.alloc(np);
+  grad.alloc(np);
+  m.alloc(np);
+  v.alloc(np);
+  TABI_CUDA(cudaMemcpyAsync(theta.p, th.data(), sizeof(float) * np, cudaMemcpyHostToDevice,
+                            stream));
+  TABI_CUDA(cudaMemsetAsync(m.p, 0, sizeof(float) * np, stream));
+  TABI_CUDA(cudaMemsetAsync(v.p, 0, sizeof(float) * np, stream));
+  ws_to_bf16_kernel<<<256, 256, 0, stream>>>(np, theta.p, wbf.p);
+  TABI_CUDA(cudaGetLastError());
+  TABI_CUDA(cudaStreamSynchronize(stream));
+}
+
+WsNet::~WsNet() {
+  if (stream) {
+    cudaStreamSynchronize(stream);
+    cudaStreamDestroy(stream);
+  }
+  if (h_stats) cudaFreeHost(h_stats);
+}
+
+std::unique_ptr<WsNet> WsNet::clone() const {
+  auto c = std::make_unique<WsNet>(H, L, 0ULL);
+  TABI_CUDA(cudaMemcpyAsync(c->theta.p, theta.p, sizeof(float) * np, cudaMemcpyDeviceToDevice,
+                            c->stream));
+  ws_to_bf16_kernel<<<256, 256, 0, c->stream>>>(np, c->theta.p, c->wbf.p);
+  TABI_CUDA(cudaGetLastError());
+  TABI_CUDA(cudaStreamSynchronize(c->stream));
+  return c;
+}
+
+void WsNet::set_params(const float* th) {
+  TABI_CUDA(cudaMemcpyAsync(theta.p, th, sizeof(float) * np, cudaMemcpyHostToDevice, stream));
+  ws_to_bf16_kernel<<<256, 256, 0, stream>>>(np, theta.p, wbf.p);
+  TABI_CUDA(cudaGetLastError());
+  adam_t = 0;
+  TABI_CUDA(cudaMemsetAsync(m.p, 0, sizeof(float) * np, stream));
+  TABI_CUDA(cudaMemsetAsync(v.p, 0, sizeof(float) * np, stream));
+  TABI_CUDA(cudaStreamSynchronize(stream));
+}
+
+void WsNet::get_params(float* th) {
+  TABI_CUDA(cudaMemcpyAsync(th, theta.p, sizeof(float) * np, cudaMemcpyDeviceToHost, stream));
+  TABI_CUDA(cudaStreamSynchronize(stream));
+}
+
+void WsNet::graph(const WsInput& in, cudaStream_t s) {
+  const int n = in.n;
+  TABI_REQUIRE(n > kK, TABI_ERR_ARG, "the warm start needs more than 16 panels");
+  pos.alloc(n);
+  nrm.alloc(n);
+  bfl.alloc(n);
+  const int pb = 148;
+  stats_part.alloc(8 * pb + 8);
+  stats.alloc(16);
+  ws_prep_kernel<<<pb, 256, 0, s>>>(n, in.px, in.py, in.pz, in.ps, in.qx, in.qy, in.qz, in.qs,
+                                     in.area, in.b, pos.p, nrm.p, bfl.p, stats_part.p);
+  ws_prep_final_kernel<<<1, 32, 0, s>>>(stats_part.p, pb, stats.p);
+  TABI_CUDA(cudaMemcpyAsync(h_stats, stats.p, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));
+  TABI_CUDA(cudaStreamSynchronize(s));
+  const double abar = h_stats[0] / n;
+  TABI_REQUIRE(abar > 0.0 && std::isfinite(h_stats[1]), TABI_ERR_ARG,
+               "warm start: panel areas must be positive and b finite");
+  // cells of ~2K panels' worth of area: the K nearest lie within a few cells
+  Grid g;
+  g.x0 = (float)h_stats[2];
+  g.y0 = (float)h_stats[3];
+  g.z0 = (float)h_stats[4];
+  const double ext[3] = {h_stats[5] - h_stats[2], h_stats[6] - h_stats[3],
+                         h_stats[7] - h_stats[4]};
+  double h = std::sqrt(2.0 * kK * abar / kPi);
+  auto dims = [&](double hh, int d) { return std::max(1, (int)std::ceil(ext[d] / hh + 1e-6)); };
+  while ((double)dims(h, 0) * dims(h, 1) * dims(h, 2) > 8.0e6) h *= 1.25;
+  g.h = (float)h;
+  g.nx = dims(h, 0);
+  g.ny = dims(h, 1);
+  g.nz = dims(h, 2);
+  const int nc = g.nx * g.ny * g.nz;
+  cell.alloc(n);
+  ccnt.alloc(nc + 1);
+  coff.alloc(nc + 1);
+  csorted.alloc(n);
+  const int sb = ceil_div(nc, kScanB);
+  const int rb = ceil_div(n, kScanB);
+  sbuf.alloc(std::max(sb, rb) + 2);
+  TABI_CUDA(cudaMemsetAsync(ccnt.p, 0, sizeof(int) * (nc + 1), s));
+  ws_cell_count_kernel<<<ceil_div(n, 256), 256, 0, s>>>(n, pos.p, g, cell.p, ccnt.p);
+  ws_scan_block_kernel<<<sb, kScanB, 0, s>>>(ccnt.p, nc, coff.p, sbuf.p);
+  ws_scan_sums_kernel<<<1, 32, 0, s>>>(sbuf.p, sb, sbuf.p + sb);
+  ws_scan_add_kernel<<<sb, kScanB, 0, s>>>(coff.p, nc, sbuf.p, sbuf.p + sb);
+  TABI_CUDA(cudaMemcpyAsync(ccnt.p, coff.p, sizeof(int) * nc, cudaMemcpyDeviceToDevice, s));
+  ws_cell_fill_kernel<<<ceil_div(n, 256), 256, 0, s>>>(n, cell.p, ccnt.p, csorted.p);
+  nbr.alloc((size_t)n * kK);
+  err.alloc(1);
+  TABI_CUDA(cudaMemsetAsync(err.p, 0, sizeof(int), s));
+  ws_knn_kernel<<<ceil_div(n, 128), 128, 0, s>>>(n, pos.p, g, coff.p, csorted.p, nbr.p, err.p);
+  // reversed lists
+  rcnt.alloc(n + 1);
+  roff.alloc(n + 1);
+  rev.alloc((size_t)n * kK);
+  TABI_CUDA(cudaMemsetAsync(rcnt.p, 0, sizeof(int) * (n + 1), s));
+  ws_rev_count_kernel<<<ceil_div((int64_t)n * kK, 256), 256, 0, s>>>(n, nbr.p, rcnt.p);
+  ws_scan_block_kernel<<<rb, kScanB, 0, s>>>(rcnt.p, n, roff.p, sbuf.p);
+  ws_scan_sums_kernel<<<1, 32, 0, s>>>(sbuf.p, rb, sbuf.p + rb);
+  ws_scan_add_kernel<<<rb, kScanB, 0, s>>>(roff.p, n, sbuf.p, sbuf.p + rb);
+  TABI_CUDA(cudaMemcpyAsync(rcnt.p, roff.p, sizeof(int) * n, cudaMemcpyDeviceToDevice, s));
+  ws_rev_fill_kernel<<<ceil_div((int64_t)n * kK, 256), 256, 0, s>>>(n, nbr.p, rcnt.p, rev.p);
+  ws_rev_sort_kernel<<<ceil_div(n, 128), 128, 0, s>>>(n, roff.p, rev.p);
+  // node features
+  dbar.alloc(n);
+  feat.alloc((size_t)n * kF);
+  ws_node_kernel<<<ceil_div(n, 128), 128, 0, s>>>(n, pos.p, nrm.p, bfl.p, nbr.p, stats.p, dbar.p,
+                                                  feat.p);
+  TABI_CUDA(cudaGetLastError());
+}
+
+void WsNet::dw(int M, int Kd, int N, const float* A, const float* D, float* g, cudaStream_t s) {
+  const int nch = ceil_div(M, kDWChunk);
+  part.alloc((size_t)nch * Kd * N);
+  dim3 grid(ceil_div(Kd, kGM), ceil_div(N, kGN), nch);
+  ws_dw_kernel<<<grid, 256, 0, s>>>(M, Kd, N, A, Kd, D, N, part.p);
+  ws_sum_parts_kernel<<<std::min(1024, ceil_div((int64_t)Kd * N, 256)), 256, 0, s>>>(
+      part.p, nch, (int64_t)Kd * N, g);
+}
+
+void WsNet::colsum(int M, int N, const float* X, float* g, cudaStream_t s) {
+  part2.alloc((size_t)kRedB * N);
+  ws_colsum_kernel<<<kRedB, 256, 0, s>>>(M, N, X, part2.p);
+  ws_sum_parts_kernel<<<ceil_div(N, 256), 256, 0, s>>>(part2.p, kRedB, N, g);
+}
+
+void WsNet::forward(const WsInput& in, double* xout, const double* target, cudaStream_t s) {
+  const int n = in.n;
+  graph(in, s);
+  const size_t nh = (size_t)n * H;
+  hs.alloc(nh * (L + 1));
+  us.alloc(nh * L);
+  as.alloc(nh * L);
+  zs.alloc(nh * L);
+  pre0.alloc(nh);
+  const __nv_bfloat16* W = wbf.p;
+  const float* T = theta.p;
+  gemm<false, 3>(n, H, kF, feat.p, kF, W + off_W0, H, T + off_b0, hs.p, H, pre0.p, nullptr, s);
+  for (int l = 0; l < L; ++l) {
+    const Layer& y = lay[l];
+    float* h = hs.p + nh * l;
+    float* u = us.p + nh * l;
+    float* a = as.p + nh * l;
+    float* z = zs.p + nh * l;
+    gemm<false, 0>(n, H, H, h, H, W + y.Wa, H, nullptr, u, H, nullptr, nullptr, s);
+    ws_agg_fwd_kernel<<<ceil_div(n, kWsNodes), H, 0, s>>>(n, H, pos.p, nrm.p, dbar.p, nbr.p,
+                                                           W + y.Wf, T + y.bf, u, a);
+    gemm<false, 1>(n, H, H, h, H, W + y.Wb1, H, T + y.bb, z, H, nullptr, nullptr, s);
+    gemm<false, 4>(n, H, H, a, H, W + y.Wb2, H, nullptr, h + nh, H, z, h, s);
+  }
+  dout.alloc(2 * (size_t)n);
+  lpart.alloc(kRedB + 2);
+  ws_head_kernel<<<kRedB, 256, 0, s>>>(n, H, hs.p + nh * L, W + off_Wo, T + off_bo, in.b, stats.p,
+                                       xout, target, dout.p, lpart.p);
+  if (target) ws_loss_final_kernel<<<1, 32, 0, s>>>(lpart.p, kRedB, n, lpart.p + kRedB);
+  TABI_CUDA(cudaGetLastError());
+}
+
+void WsNet::backward(int n, cudaStream_t s) {
+  const size_t nh = (size_t)n * H;
+  dh.alloc(nh);
+  dz.alloc(nh);
+  da.alloc(nh);
+  du.alloc(nh);
+  wpart.alloc((size_t)kWsBlocks * (kE + 1) * H);
+  float* G = grad.p;
+  const __nv_bfloat16* W = wbf.p;
+  const float* T = theta.p;
+  TABI_CUDA(cudaMemsetAsync(G, 0, sizeof(float) * np, s));
+  // head
+  dw(n, H, 2, hs.p + nh * L, dout.p, G + off_Wo, s);
+  colsum(n, 2, dout.p, G + off_bo, s);
+  ws_head_bwd_kernel<<<1024, 256, 0, s>>>(n, H, dout.p, W + off_Wo, dh.p);
+  const int eb = 1024;
+  for (int l = L - 1; l >= 0; --l) {
+    const Layer& y = lay[l];
+    const float* hin = hs.p + nh * l;
+    const float* u = us.p + nh * l;
+    const float* a = as.p + nh * l;
+    const float* z = zs.p + nh * l;
+    ws_dsilu_kernel<<<eb, 256, 0, s>>>((int64_t)nh, dh.p, z, dz.p);
+    dw(n, H, H, hin, dz.p, G + y.Wb1, s);
+    dw(n, H, H, a, dz.p, G + y.Wb2, s);
+    colsum(n, H, dz.p, G + y.bb, s);
+    // dh_in = dh + dz Wb1^T ; da = dz Wb2^T
+    gemm<true, 2>(n, H, H, dz.p, H, W + y.Wb1, H, nullptr, dh.p, H, nullptr, nullptr, s);
+    gemm<true, 0>(n, H, H, dz.p, H, W + y.Wb2, H, nullptr, da.p, H, nullptr, nullptr, s);
+    // aggregation: Wf (kE x H) and bf (H) are adjacent in the flat layout
+    ws_agg_bwd_w_kernel<<<kWsBlocks, H, 0, s>>>(n, H, pos.p, nrm.p, dbar.p, nbr.p, W + y.Wf,
+                                                T + y.bf, u, da.p, wpart.p);
+    ws_sum_parts_kernel<<<ceil_div((int64_t)(kE + 1) * H, 256), 256, 0, s>>>(
+        wpart.p, kWsBlocks, (int64_t)(kE + 1) * H, G + y.Wf);
+    ws_agg_bwd_u_kernel<<<ceil_div(n, kWsNodes), H, 0, s>>>(n, H, pos.p, nrm.p, dbar.p, roff.p,
+                                                             rev.p, W + y.Wf, T + y.bf, da.p,
+                                                             du.p);
+    dw(n, H, H, hin, du.p, G + y.Wa, s);
+    gemm<true, 2>(n, H, H, du.p, H, W + y.Wa, H, nullptr, dh.p, H, nullptr, nullptr, s);
+  }
+  // input layer
+  ws_dsilu_kernel<<<eb, 256, 0, s>>>((int64_t)nh, dh.p, pre0.p, dz.p);
+  dw(n, kF, H, feat.p, dz.p, G + off_W0, s);
+  colsum(n, H, dz.p, G + off_b0, s);
+  TABI_CUDA(cudaGetLastError());
+}
+
+void WsNet::adam(double lr, cudaStream_t s) {
+  ++adam_t;
+  const float b1 = 0.9f, b2 = 0.999f;
+  const float c1 = 1.f - std::pow(b1, (float)adam_t), c2 = 1.f - std::pow(b2, (float)adam_t);
+  ws_adam_kernel<<<256, 256, 0, s>>>(np, theta.p, grad.p, m.p, v.p, (float)lr, b1, b2, c1, c2,
+                                     1e-8f, wbf.p);
+  TABI_CUDA(cudaGetLastError());
+}
+
+double WsNet::read_loss(cudaStream_t s) {
+  TABI_CUDA(cudaMemcpyAsync(h_stats + 8, lpart.p + kRedB, sizeof(double), cudaMemcpyDeviceToHost,
+                            s));
+  TABI_CUDA(cudaStreamSynchronize(s));
+  return h_stats[8];
+}
+
+bool WsNet::graph_exact(cudaStream_t s) {
+  int e = 0;
+  TABI_CUDA(cudaMemcpyAsync(&h_stats[9], err.p, sizeof(int), cudaMemcpyDeviceToHost, s));
+  TABI_CUDA(cudaStreamSynchronize(s));
+  std::memcpy(&e, &h_stats[9], sizeof(int));
+  return e == 0;
+}
+
+}  // namespace tabi

@@ -30,6 +30,9 @@ SYMBOLS = [
     "tabi_energy", "tabi_energy_dev", "tabi_run_dev", "tabi_counts", "tabi_tree_nodes",
     "tabi_probe_fp64_peak", "tabi_profile_enable", "tabi_profile_read", "tabi_profile_nclasses",
     "tabi_profile_class_name", "tabi_energy_noalloc",
+    "tabi_ws_create", "tabi_ws_destroy", "tabi_ws_nparams", "tabi_ws_get_params",
+    "tabi_ws_set_params", "tabi_ws_predict_dev", "tabi_ws_loss_grad_dev",
+    "tabi_ws_train_step_dev", "tabi_ws_graph_dev", "tabi_set_warmstart", "tabi_batch_run_dev",
 ]
 
 
@@ -50,6 +53,16 @@ class Params(C.Structure):
                 ("iprcd", C.c_int), ("tol", C.c_double), ("maxl", C.c_int), ("nrmax", C.c_int),
                 ("precision", C.c_int), ("flags", C.c_int)]
 
+
+class MolDev(C.Structure):
+    """tabi_mol_dev (include/tabi_gpu.h): one molecule of a batch."""
+    _fields_ = [("nspt", C.c_int), ("sptpos", C.c_void_p), ("sptnrm", C.c_void_p),
+                ("nface", C.c_int), ("nvert", C.c_void_p), ("nchr", C.c_int),
+                ("chrpos", C.c_void_p), ("atmchr", C.c_void_p), ("maxparnode", C.c_int),
+                ("order", C.c_int)]
+
+
+BATCH_STATS = 12
 
 _lib = None
 _dp = C.POINTER(C.c_double)
@@ -98,10 +111,25 @@ def load(path: str = LIB_PATH):
     L.tabi_profile_class_name.restype = C.c_char_p
     L.tabi_energy_noalloc.argtypes = [C.c_int, _vp, _vp, _vp, _vp, C.c_int, _vp, _vp, C.c_double,
                                       C.c_double, C.c_double, _vp, _vp]
+    _fp = C.POINTER(C.c_float)
+    L.tabi_ws_create.argtypes = [C.POINTER(_vp), C.c_int, C.c_int, C.c_ulonglong]
+    L.tabi_ws_destroy.argtypes = [_vp]
+    L.tabi_ws_nparams.argtypes = [_vp]
+    L.tabi_ws_get_params.argtypes = [_vp, _fp, C.c_longlong]
+    L.tabi_ws_set_params.argtypes = [_vp, _fp, C.c_longlong]
+    L.tabi_ws_predict_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.tabi_ws_loss_grad_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _dp, _fp, _vp]
+    L.tabi_ws_train_step_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_double,
+                                         _dp, _vp]
+    L.tabi_ws_graph_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _ip, _fp, _vp]
+    L.tabi_set_warmstart.argtypes = [_vp, _vp]
+    L.tabi_batch_run_dev.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(MolDev), _vp, C.c_int,
+                                     _dp]
     for s in SYMBOLS:
         if s not in ("tabi_default_params", "tabi_kappa", "tabi_last_error",
-                     "tabi_profile_class_name"):
+                     "tabi_profile_class_name", "tabi_ws_nparams"):
             getattr(L, s).restype = C.c_int
+    L.tabi_ws_nparams.restype = C.c_longlong
     _lib = L
     return L
 

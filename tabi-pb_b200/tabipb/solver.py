@@ -208,6 +208,12 @@ class TabiSolver:
     def matvec_dev(self, x_ptr, y_ptr, n2, stream=None):
         check(self.h, self.L.tabi_matvec_dev(self.h, n2, x_ptr, y_ptr, stream))
 
+    def set_warmstart(self, ws):
+        """Attach a warmstart.WarmStart (None detaches): run_dev then starts
+        GMRES from the network's prediction (tabi_set_warmstart)."""
+        check(self.h, self.L.tabi_set_warmstart(self.h, ws.h if ws is not None else None))
+        self._ws = ws  # the handle does not own the network
+
     def run_dev(self, nspt, sptpos_ptr, sptnrm_ptr, nface, nvert_ptr, nchr, chrpos_ptr,
                 atmchr_ptr, x_ptr=None, stream=None):
         st = np.zeros(8)

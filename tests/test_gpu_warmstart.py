@@ -1,0 +1,130 @@
+"""Learned warm start (tabi_ws_*): the CUDA network against its CPU reference
+(oracle/warmstart_ref.py), and what a trained network gains.
+
+Bars: neighbour lists equal to a brute-force search except at distance ties
+within FP32 rounding; node features, prediction, loss and gradient within
+FP32-accumulation tolerance of the FP64 reference computed with the same
+bfloat16 weights; a network trained on a handful of solved molecules lowers
+the GMRES iteration count on held-out molecules, with the solve still meeting
+its tolerance.
+"""
+import numpy as np
+import pytest
+
+from conftest import molecule_case
+
+pytestmark = pytest.mark.gpu
+
+
+def _sample(case, dev):
+    import torch
+
+    import oracle as O
+
+    xyz, tq, ar, b = O.form_matrix(case["sptpos"], case["sptnrm"], case["nvert"],
+                                   case["chrpos"], case["atmchr"], 1.0)
+    t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64).ravel()).to(dev)
+    rng = np.random.default_rng(3)
+    x = b * 0.3 + rng.standard_normal(b.size) * np.std(b) * 0.1
+    return dict(n=len(ar), xyz=t(xyz), tq=t(tq), area=t(ar), b=t(b), x=t(x)), (xyz, tq, ar, b, x)
+
+
+@pytest.fixture(scope="module")
+def small(gpu_lib):
+    import torch
+
+    case = molecule_case(60, 6.0, 2.0, seed=1)
+    return _sample(case, torch.device("cuda", 0))
+
+
+def test_graph_and_features_match_reference(small):
+    import warmstart_ref as W
+
+    from tabipb.warmstart import WarmStart
+
+    s, (xyz, tq, ar, b, x) = small
+    ws = WarmStart(hidden=32, layers=1, seed=0)
+    nbr, feat = ws.graph_dev(s)
+    ref = W.knn(xyz, 16)
+    pos = xyz.reshape(-1, 3)
+    d = lambda i, js: np.sqrt(((pos[js] - pos[i]) ** 2).sum(-1))
+    bad = 0
+    for i in range(len(ar)):
+        if set(nbr[i]) != set(ref[i]):
+            # only a tie at the K-th distance (FP32 vs FP64 ordering) may differ
+            assert abs(d(i, nbr[i]).max() - d(i, ref[i]).max()) <= 1e-5 * d(i, ref[i]).max(), i
+            bad += 1
+    assert bad <= len(ar) // 100
+    f_ref, _, _ = W.features(pos, tq.reshape(-1, 3), ar, b, nbr.astype(np.int64), 8)
+    rest = [0, 1, 2, 3, 5, 6, 7]
+    np.testing.assert_allclose(feat[:, rest], f_ref[:, rest], rtol=2e-4, atol=2e-5)
+    # the curvature feature divides n.(r_j - r_i) by |r_j - r_i|^2: for nearly
+    # coincident centroids it amplifies the FP32 rounding of the positions
+    np.testing.assert_allclose(feat[:, 4], f_ref[:, 4], rtol=0,
+                               atol=1e-2 * np.abs(f_ref[:, 4]).max())
+
+
+def test_loss_gradient_prediction_match_reference(small):
+    import torch
+    import warmstart_ref as W
+
+    from tabipb.warmstart import WarmStart
+
+    s, (xyz, tq, ar, b, x) = small
+    H, L, R = 32, 2, 8
+    ws = WarmStart(hidden=H, layers=L, seed=0)
+    theta = W.init_params(H, L, R, seed=4)
+    ws.set_params(theta)
+    nbr, _ = ws.graph_dev(s)
+    nbr = nbr.astype(np.int64)
+    pos, nrm = xyz.reshape(-1, 3), tq.reshape(-1, 3)
+    xr, loss_ref, cache = W.forward(theta, H, L, R, pos, nrm, ar, b, nbr, target=x)
+    g_ref = W.backward(cache, H, L, R, nbr)
+    loss, g = ws.loss_grad_dev(s)
+    assert abs(loss - loss_ref) <= 1e-4 * abs(loss_ref), (loss, loss_ref)
+    # per parameter tensor: relative to the tensor's largest gradient
+    o = 0
+    for name, shp in W.param_shapes(H, L, R):
+        k = int(np.prod(shp))
+        gr, gg = g_ref[o:o + k], g[o:o + k]
+        scale = np.abs(gr).max() + 1e-30
+        assert np.abs(gg - gr).max() <= 2e-3 * scale, (name, np.abs(gg - gr).max(), scale)
+        o += k
+    xp = torch.empty_like(s["b"])
+    ws.predict_dev(s, xp)
+    xp = xp.cpu().numpy()
+    assert np.linalg.norm(xp - xr) <= 1e-4 * np.linalg.norm(xr)
+
+
+def test_training_step_is_deterministic(small):
+    from tabipb.warmstart import WarmStart
+
+    s, _ = small
+    out = []
+    for _ in range(2):
+        ws = WarmStart(hidden=32, layers=2, seed=7)
+        for k in range(3):
+            ws.train_step_dev(s, 1e-3)
+        out.append(ws.params())
+    assert np.array_equal(out[0], out[1])
+
+
+def test_trained_network_cuts_iterations(gpu_lib):
+    """Train on 12 small solved molecules, evaluate on 4 held-out ones."""
+    from tabipb import warmstart as WS
+
+    train_set = [WS.make_sample(int(na), seed=100 + k, density=3.0, tol=1e-6)
+                 for k, na in enumerate(np.geomspace(150, 500, 12).astype(int))]
+    test_set = [WS.make_sample(300, seed=900 + k, density=3.0, tol=1e-6) for k in range(4)]
+    ws = WS.WarmStart(hidden=160, layers=3, seed=0)
+    assert ws.nparams == 238402
+    hist = WS.train(ws, train_set, epochs=25, lr=2e-3, lr_final=2e-4)
+    assert hist[-1] < 0.5 * hist[0], hist
+    ev = WS.evaluate(ws, test_set, tol=1e-6)
+    for e in ev:
+        assert e["ierr"] == (0, 0), e
+    it0 = np.mean([e["iters_zero"] for e in ev])
+    itw = np.mean([e["iters_ws"] for e in ev])
+    print("iterations from zero", it0, "from the network", itw,
+          "x0 error", [round(e["x0_rel_err"], 3) for e in ev], "loss", hist[0], hist[-1])
+    assert itw < it0, (itw, it0)
