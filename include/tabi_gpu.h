@@ -220,8 +220,9 @@ int tabi_probe_fp64_peak(double ms, double* flops);
  * network trains on the GPU (its own forward, backward and Adam kernels) on
  * solutions of this solver.  All surface arrays are device pointers in the
  * reference's layout (tr_xyz, tr_q 3 x nface, tr_area nface, bvct and x
- * 2 nface), in any one face order; stream NULL = the network's own stream.
- * A network object is not thread-safe. */
+ * 2 nface), in any one face order.  The _dev calls are ordered on `stream`
+ * (NULL = the CUDA default stream); the loss / graph calls return after their
+ * results are on the host.  A network object is not thread-safe. */
 typedef struct tabi_ws_s* tabi_ws;
 
 /* hidden: multiple of 32 in 32..256; layers 1..8; deterministic init from

@@ -728,9 +728,8 @@ int tabi_probe_fp64_peak(double ms, double* flops) {
 }
 
 // ---- learned warm start
-static cudaStream_t ws_stream(tabi_ws w, void* stream) {
-  return stream ? (cudaStream_t)stream : w->net->stream;
-}
+// NULL = the CUDA default stream, as for any CUDA call
+static cudaStream_t ws_stream(tabi_ws, void* stream) { return (cudaStream_t)stream; }
 
 int tabi_ws_create(tabi_ws* w, int hidden, int layers, unsigned long long seed) {
   if (!w) return TABI_ERR_ARG;

@@ -34,6 +34,17 @@ def _ptr(t):
     return C.c_void_p(t.data_ptr()) if t is not None else None
 
 
+def _stream(stream):
+    """The stream a call runs on: the given one, else torch's current stream
+    (so the call is ordered with the torch operations around it; torch's
+    default stream is the CUDA default stream, NULL)."""
+    if stream is not None:
+        return C.c_void_p(stream)
+    import torch
+
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
 class WarmStart:
     """One network (tabi_ws); see include/tabi_gpu.h."""
 
@@ -90,7 +101,7 @@ class WarmStart:
     def predict_dev(self, s, x_out, stream=None):
         self._check(self.L.tabi_ws_predict_dev(self.h, s["n"], _ptr(s["xyz"]), _ptr(s["tq"]),
                                                _ptr(s["area"]), _ptr(s["b"]), _ptr(x_out),
-                                               stream))
+                                               _stream(stream)))
 
     def loss_grad_dev(self, s, want_grad=True, stream=None):
         loss = C.c_double()
@@ -98,14 +109,14 @@ class WarmStart:
         self._check(self.L.tabi_ws_loss_grad_dev(
             self.h, s["n"], _ptr(s["xyz"]), _ptr(s["tq"]), _ptr(s["area"]), _ptr(s["b"]),
             _ptr(s["x"]), C.byref(loss),
-            g.ctypes.data_as(C.POINTER(C.c_float)) if g is not None else None, stream))
+            g.ctypes.data_as(C.POINTER(C.c_float)) if g is not None else None, _stream(stream)))
         return loss.value, g
 
     def train_step_dev(self, s, lr, stream=None):
         loss = C.c_double()
         self._check(self.L.tabi_ws_train_step_dev(
             self.h, s["n"], _ptr(s["xyz"]), _ptr(s["tq"]), _ptr(s["area"]), _ptr(s["b"]),
-            _ptr(s["x"]), float(lr), C.byref(loss), stream))
+            _ptr(s["x"]), float(lr), C.byref(loss), _stream(stream)))
         return loss.value
 
     def graph_dev(self, s, stream=None):
@@ -115,7 +126,7 @@ class WarmStart:
         self._check(self.L.tabi_ws_graph_dev(
             self.h, n, _ptr(s["xyz"]), _ptr(s["tq"]), _ptr(s["area"]), _ptr(s["b"]),
             nbr.ctypes.data_as(C.POINTER(C.c_int)), feat.ctypes.data_as(C.POINTER(C.c_float)),
-            stream))
+            _stream(stream)))
         return nbr, feat
 
 

