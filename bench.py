@@ -51,6 +51,8 @@ METRIC = "solves/s (TABI-PB solve at <=1e-4 dG error; plain FP64)"
 # GMRES iterations of this workload, from the parity-checked GPU run (the
 # oracle reproduces the GPU's iteration count; used to scale the CPU sample)
 WORKLOAD_ITERS = None
+# trained warm-start network (tabipb.train_warmstart)
+WEIGHTS = os.path.join(ROOT, "tabi-pb_b200", "weights", "warmstart_h160_l3.npz")
 OPS_NEAR_PAIR = 64  # algorithmic ops per near-field pair (reference formulas)
 
 
@@ -257,46 +259,63 @@ def gpu_arm(args):
 
     # ---- the same solve with the mixed-precision operator (FP32 treecode,
     # FP64 refinement): same workload, tol, flush and timing
-    mixed = None
-    if not args.no_mixed:
-        msolver = tabipb.TabiSolver(order=w["order"], maxparnode=w["maxparnode"],
-                                    theta=w["theta"], kappa=kap, eps0=w["eps0"], eps1=w["eps1"],
-                                    tol=w["tol"], precision=tabipb.PREC_MIXED)
-
-        def mstep():
-            return msolver.run_dev(nspt, d["sptpos"].data_ptr(), d["sptnrm"].data_ptr(), nface,
-                                   d["nvert"].data_ptr(), natm, d["chrpos"].data_ptr(),
-                                   d["atmchr"].data_ptr(), None, sp)
+    def timed_leg(solver):
+        """The timed loop of the main leg, on another solver configuration."""
+        def st():
+            return solver.run_dev(nspt, d["sptpos"].data_ptr(), d["sptnrm"].data_ptr(), nface,
+                                  d["nvert"].data_ptr(), natm, d["chrpos"].data_ptr(),
+                                  d["atmchr"].data_ptr(), None, sp)
 
         for _ in range(args.warmup):
-            mres = mstep()
+            r = st()
         torch.cuda.synchronize()
-        msolver.profile(True)
-        mtimes = []
+        solver.profile(True)
+        tt = []
         for _ in range(args.steps):
             flush.zero_()
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            mres = mstep()
+            r = st()
             e1.record(stream)
-            mtimes.append((e0, e1))
+            tt.append((e0, e1))
         torch.cuda.synchronize()
-        mms = sum(a.elapsed_time(b) for a, b in mtimes)
-        mprof = msolver.profile_read()
-        msolver.close()
-        mms_t = torch.tensor([mms], dtype=torch.float64, device=dev)
+        lms = sum(a.elapsed_time(b) for a, b in tt)
+        lprof = solver.profile_read()
+        solver.profile(False)
+        lms_t = torch.tensor([lms], dtype=torch.float64, device=dev)
         if world > 1:
-            dist.all_reduce(mms_t, op=dist.ReduceOp.MAX)
-        mms = float(mms_t.item())
-        mixed = {"value": world * args.steps / (mms / 1e3), "unit": "solves/s",
-                 "ms_per_step": mms / args.steps, "gmres_iterations": mres["iter"],
-                 "fp64_residual_measure": mres["err"], "ierr": mres["ierr"],
-                 "soleng_kcal_mol": mres["soleng"],
-                 "dG_rel_diff_vs_fp64": abs(mres["soleng"] - res["soleng"]) / abs(res["soleng"]),
-                 "phase_ms_per_step": {k: v[0] / args.steps for k, v in mprof.items()
-                                       if k != "all"},
-                 "gpu_launches": int(mprof["all"][1])}
+            dist.all_reduce(lms_t, op=dist.ReduceOp.MAX)
+        lms = float(lms_t.item())
+        return {"value": world * args.steps / (lms / 1e3), "unit": "solves/s",
+                "ms_per_step": lms / args.steps, "gmres_iterations": r["iter"],
+                "fp64_residual_measure": r["err"], "ierr": r["ierr"],
+                "soleng_kcal_mol": r["soleng"],
+                "dG_rel_diff_vs_fp64": abs(r["soleng"] - res["soleng"]) / abs(res["soleng"]),
+                "phase_ms_per_step": {k: v[0] / args.steps for k, v in lprof.items()
+                                      if k != "all"},
+                "gpu_launches": int(lprof["all"][1])}
+
+    # ---- the same solve with the mixed-precision operator (FP32 treecode,
+    # FP64 refinement), and with the learned warm start on top
+    mixed = learned = None
+    if not args.no_mixed:
+        msolver = tabipb.TabiSolver(order=w["order"], maxparnode=w["maxparnode"],
+                                    theta=w["theta"], kappa=kap, eps0=w["eps0"], eps1=w["eps1"],
+                                    tol=w["tol"], precision=tabipb.PREC_MIXED)
+        mixed = timed_leg(msolver)
+        if os.path.exists(WEIGHTS):
+            from tabipb.warmstart import WarmStart
+
+            ws = WarmStart.load(WEIGHTS)
+            msolver.set_warmstart(ws)
+            learned = timed_leg(msolver)
+            learned["weights"] = os.path.relpath(WEIGHTS, ROOT)
+            msolver.set_warmstart(None)
+            ws.close()
+        else:
+            learned = {"unavailable": "no trained weights at " + os.path.relpath(WEIGHTS, ROOT)}
+        msolver.close()
 
     # ---- end to end through the host-array C ABI: one handle (one molecule
     # at a time, buffers reused), host arrays in and out every step
@@ -334,6 +353,8 @@ def gpu_arm(args):
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_s = float(e2e_t.item())
     e2e_solver.close()
+
+    batched = batched_leg(args, dev, rank) if args.batch > 0 else None
 
     out = None
     if rank == 0:
@@ -387,6 +408,9 @@ def gpu_arm(args):
         }
         if mixed is not None:
             out["mixed"] = mixed
+            out["mixed_learned"] = learned
+        if batched is not None:
+            out["batched"] = batched
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -398,6 +422,79 @@ def gpu_arm(args):
     if out is not None:
         print(json.dumps(out), flush=True)
     solver.close()
+
+
+# ---------------------------------------------------------------- batched leg
+def _batch_surface(job):
+    natm, seed, density = job
+    from tabipb import surface as S
+    from tabipb.warmstart import globular_radius
+
+    xyz, q, r = S.synthetic_molecule(natm, globular_radius(natm), min_sep=2.0, seed=seed)
+    pos, nrm, fc, _ = S.gaussian_surface(xyz, r, density=density, probe=1.4)
+    fc, _ = S.face_filter(pos, fc)
+    return natm, seed, pos, nrm, fc, xyz, q
+
+
+def batched_leg(args, dev, rank):
+    """Many molecules of uneven size in one tabi_batch_run_dev call: atom counts
+    log-uniform in 300..8000 (seeded; rank r uses seeds r*1000 + k), the
+    benchmark's atom density and surface density, mixed precision, tol 1e-4,
+    leaf size per size class from the autotuner, the trained warm start when
+    its weights exist.  Reported: molecules/s of the whole batch on
+    --batch-workers workers and on one (the same molecules back to back), and
+    the per-molecule wall-time percentiles."""
+    import multiprocessing as mp
+
+    import torch
+
+    import tabipb
+    from tabipb import batch as B
+
+    rng = np.random.default_rng(7 + rank)
+    sizes = np.exp(rng.uniform(np.log(300), np.log(8000), args.batch)).astype(int)
+    jobs = [(int(n), rank * 1000 + k, 10.0) for k, n in enumerate(sizes)]
+    t0 = time.perf_counter()
+    with mp.get_context("spawn").Pool(min(16, os.cpu_count() or 1)) as pool:
+        hosts = pool.map(_batch_surface, jobs, chunksize=1)
+    t_gen = time.perf_counter() - t0
+    f = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)).to(dev)
+    mols = [dict(natm=n, seed=sd, nspt=len(pos), nface=len(fc), nchr=n, sptpos=f(pos),
+                 sptnrm=f(nrm), nvert=torch.from_numpy(np.ascontiguousarray(fc, np.int32)).to(dev),
+                 chrpos=f(xyz), atmchr=f(q)) for n, sd, pos, nrm, fc, xyz, q in hosts]
+    w = WORKLOAD
+    prm = tabipb.default_params(order=w["order"], theta=w["theta"], maxparnode=w["maxparnode"],
+                                kappa=tabipb.kappa(w["bulk"], w["eps1"]), eps0=w["eps0"],
+                                eps1=w["eps1"], tol=w["tol"], precision=tabipb.PREC_MIXED)
+    # autotune the leaf size on one probe molecule per size class present
+    probes = {}
+    for m in mols:
+        probes.setdefault(B.size_class(m["nface"]), m)
+    table, timings = B.autotune(list(probes.values()), prm, candidates=(300, 500, 700),
+                                repeats=1)
+    ws = None
+    if os.path.exists(WEIGHTS):
+        from tabipb.warmstart import WarmStart
+
+        ws = WarmStart.load(WEIGHTS)
+    B.run_batch(mols[:2], prm, ws=ws, nworkers=2, table=table)  # warm-up
+    seq, t_seq = B.run_batch(mols, prm, ws=ws, nworkers=1, table=table)
+    par, t_par = B.run_batch(mols, prm, ws=ws, nworkers=args.batch_workers, table=table)
+    ok = bool(np.all(par[:, 2] == 0)) and bool(np.array_equal(seq[:, 3], par[:, 3]))
+    return {"value": len(mols) / t_par, "unit": "molecules/s", "molecules": len(mols),
+            "workers": args.batch_workers,
+            "sequential_value": len(mols) / t_seq,
+            "speedup_vs_sequential": t_seq / t_par,
+            "faces_min_max": [int(min(m["nface"] for m in mols)),
+                              int(max(m["nface"] for m in mols))],
+            "atoms": "log-uniform 300..8000, seeded", "precision": "mixed", "tol": w["tol"],
+            "warm_start": ws is not None,
+            "leaf_table": {str(k): v for k, v in table.items()},
+            "per_molecule_ms_p50": float(np.percentile(par[:, 8], 50)),
+            "per_molecule_ms_p99": float(np.percentile(par[:, 8], 99)),
+            "all_converged_and_equal_to_sequential": ok,
+            "timing": "host wall clock around the whole batch call (inputs on the device)",
+            "surface_generation_s": t_gen}
 
 
 # ---------------------------------------------------------------- reference arm
@@ -445,6 +542,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision leg (FP32 treecode + FP64 refinement)")
+    ap.add_argument("--batch", type=int, default=16,
+                    help="molecules in the batched leg (0 skips it)")
+    ap.add_argument("--batch-workers", type=int, default=4)
     ap.add_argument("--iters", type=int, default=27,
                     help="GMRES iterations used to scale the reference-arm sample")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="globular")

@@ -217,6 +217,10 @@ int tabi_probe_fp64_peak(double ms, double* flops);
  * matrices with FP32 accumulation) predicts x0 = [phi; dphi/dn] from the
  * panel geometry and the right-hand side; GMRES on the true residual then
  * runs from x0, so the prediction changes the iteration count only.  The
+ * network corrects zprec = M^-1 bvct, the leaf-block preconditioner's solution
+ * (tabi_msolve of the right-hand side; it solves the equations exactly within
+ * each leaf), which is also one of its inputs; zprec may be NULL, the
+ * baseline is then [0; b2].  The
  * network trains on the GPU (its own forward, backward and Adam kernels) on
  * solutions of this solver.  All surface arrays are device pointers in the
  * reference's layout (tr_xyz, tr_q 3 x nface, tr_area nface, bvct and x
@@ -226,7 +230,7 @@ int tabi_probe_fp64_peak(double ms, double* flops);
 typedef struct tabi_ws_s* tabi_ws;
 
 /* hidden: multiple of 32 in 32..256; layers 1..8; deterministic init from
- * seed (output layer zero: an untrained network predicts x1 = 0, x2 = b2). */
+ * seed (output layer zero: an untrained network predicts the baseline). */
 int tabi_ws_create(tabi_ws* w, int hidden, int layers, unsigned long long seed);
 int tabi_ws_destroy(tabi_ws w);
 /* number of FP32 parameters (-1 for a NULL network) */
@@ -237,28 +241,29 @@ int tabi_ws_get_params(tabi_ws w, float* theta, long long n);
 int tabi_ws_set_params(tabi_ws w, const float* theta, long long n);
 /* x0 (device, 2 nface) = the network's prediction */
 int tabi_ws_predict_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
-                        const double* tr_area, const double* bvct, double* x0,
-                        void* stream);
+                        const double* tr_area, const double* bvct, const double* zprec,
+                        double* x0, void* stream);
 /* loss against a solution x_target (device, 2 nface) and, if grad != NULL,
  * its gradient with respect to the parameters (host, tabi_ws_nparams) */
 int tabi_ws_loss_grad_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
-                          const double* tr_area, const double* bvct,
+                          const double* tr_area, const double* bvct, const double* zprec,
                           const double* x_target, double* loss, float* grad,
                           void* stream);
 /* one Adam step (beta 0.9 / 0.999) on one molecule; *loss (may be NULL) =
  * the loss before the step */
 int tabi_ws_train_step_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
-                           const double* tr_area, const double* bvct,
+                           const double* tr_area, const double* bvct, const double* zprec,
                            const double* x_target, double lr, double* loss,
                            void* stream);
 /* the network's input: neighbour lists (host, nface x 16) and node features
- * (host, nface x 8); either may be NULL */
+ * (host, nface x 10); either may be NULL */
 int tabi_ws_graph_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
-                      const double* tr_area, const double* bvct, int* nbr, float* feat,
-                      void* stream);
+                      const double* tr_area, const double* bvct, const double* zprec,
+                      int* nbr, float* feat, void* stream);
 /* attaches a network to a solve handle (NULL detaches): tabi_run_dev then
- * starts GMRES from the network's prediction instead of zero.  The handle
- * does not own the network. */
+ * applies the preconditioner to the right-hand side and starts GMRES from the
+ * network's correction of it instead of zero.  The handle does not own the
+ * network. */
 int tabi_set_warmstart(tabi_h h, tabi_ws w);
 
 /* ---- Batched solves (no counterpart in the reference, which solves one

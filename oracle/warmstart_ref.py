@@ -7,14 +7,16 @@ has no learned component: this restates the network the CUDA kernels
 implement, term for term, so the two can be compared.
 
 Network ("panel network"), for one molecule of N panels (centroid r_i, unit
-normal n_i, area A_i, right-hand side b = [b1; b2] of main.f90:592-606):
+normal n_i, area A_i, right-hand side b = [b1; b2] of main.f90:592-606, and
+z = [z1; z2] = M^-1 b, the leaf-block preconditioner's solution, which solves
+the boundary integral equations exactly within each leaf; without z, z = [0; b2]):
 
   neighbours  nbr(i, :) = the K nearest other panels by centroid distance,
               ascending, ties by index
   scales      s = sqrt(mean b1^2), Abar = mean A, dbar_i = mean_k |r_j - r_i|
-  node input  f_i (8): b1_i/s, b2_i/s, log(A_i/Abar), log(Abar),
+  node input  f_i (10): b1_i/s, b2_i/s, log(A_i/Abar), log(Abar),
               mean_k n_i.(r_j - r_i) dbar_i / |r_j - r_i|^2, mean_k n_i.n_j,
-              log(dbar_i), mean_k (b1_j - b1_i)/s
+              log(dbar_i), mean_k (b1_j - b1_i)/s, asinh(z1_i/s), asinh((z2_i - b2_i)/s)
   edge input  e_ij (R + 3): exp(-((|r_ij|/dbar_i - mu_m)/sigma)^2) for
               mu_m = 2.5 m/(R-1), sigma = 2.5/(R-1); n_i.n_j; n_i.r_ij/|r_ij|;
               n_j.r_ij/|r_ij|   (r_ij = r_j - r_i)
@@ -22,8 +24,8 @@ normal n_i, area A_i, right-hand side b = [b1; b2] of main.f90:592-606):
               repeat L times:  u = h Wa
                                a_i = 1/K sum_k silu(e_ij Wf + bf) * u_j
                                z = h Wb1 + a Wb2 + bb ;  h = h + silu(z)
-  output      o = h Wo + bo ;  x1 = s o_0 ,  x2 = b2 + s o_1
-  loss        1/N sum_i (o_i0 - x1_i/s)^2 + (o_i1 - (x2_i - b2_i)/s)^2
+  output      o = h Wo + bo ;  x1 = z1 + s o_0 ,  x2 = z2 + s o_1
+  loss        1/N sum_i (o_i0 - (x1_i - z1_i)/s)^2 + (o_i1 - (x2_i - z2_i)/s)^2
 
 Every input is invariant under rotations and translations of the molecule,
 so the predicted potentials are too; scaling all charges scales s, b and the
@@ -34,7 +36,7 @@ from __future__ import annotations
 
 import numpy as np
 
-NODE_F = 8
+NODE_F = 10
 
 
 def edge_dim(R):
@@ -100,9 +102,15 @@ def knn(pos, K):
     return out
 
 
-def features(pos, nrm, area, b, nbr, R):
+def baseline(b, z):
+    n = len(b) // 2
+    return np.concatenate([np.zeros(n), b[n:]]) if z is None else np.asarray(z, np.float64)
+
+
+def features(pos, nrm, area, b, nbr, R, z=None):
     n = len(area)
     b1, b2 = b[:n], b[n:]
+    z = baseline(b, z)
     s = np.sqrt(np.mean(b1 * b1))
     if s == 0.0:
         s = 1.0
@@ -121,6 +129,8 @@ def features(pos, nrm, area, b, nbr, R):
     f[:, 5] = (ni * nj).sum(-1).mean(1)
     f[:, 6] = np.log(dbar)
     f[:, 7] = ((b1[nbr] - b1[:, None]) / s).mean(1)
+    f[:, 8] = np.arcsinh(z[:n] / s)
+    f[:, 9] = np.arcsinh((z[n:] - b2) / s)
     mu = 2.5 * np.arange(R) / (R - 1)
     sig = 2.5 / (R - 1)
     rho = d / dbar[:, None]
@@ -132,7 +142,7 @@ def features(pos, nrm, area, b, nbr, R):
     return f, e, s
 
 
-def forward(theta, H, L, R, pos, nrm, area, b, nbr, target=None, round_bf16=True):
+def forward(theta, H, L, R, pos, nrm, area, b, nbr, target=None, round_bf16=True, z=None):
     """Returns (x_pred, loss or None, cache).  round_bf16=False keeps the
     weights exact (for finite-difference checks of backward())."""
     th = np.asarray(theta, np.float32 if round_bf16 else np.float64)
@@ -140,7 +150,8 @@ def forward(theta, H, L, R, pos, nrm, area, b, nbr, target=None, round_bf16=True
          for k, v in unpack(th, H, L, R).items()}
     n = len(area)
     K = nbr.shape[1]
-    f, e, s = features(pos, nrm, area, b, nbr, R)
+    f, e, s = features(pos, nrm, area, b, nbr, R, z)
+    zb = baseline(b, z)
     pre0 = f @ p["W0"] + p["b0"]
     h = silu(pre0)
     cache = dict(f=f, e=e, s=s, pre0=pre0, hs=[h], us=[], pres=[], as_=[], zs=[], p=p)
@@ -148,20 +159,20 @@ def forward(theta, H, L, R, pos, nrm, area, b, nbr, target=None, round_bf16=True
         u = h @ p[f"Wa{l}"]
         pre = e @ p[f"Wf{l}"] + p[f"bf{l}"]            # N x K x H
         a = (silu(pre) * u[nbr]).sum(1) / K
-        z = h @ p[f"Wb1{l}"] + a @ p[f"Wb2{l}"] + p[f"bb{l}"]
-        h = h + silu(z)
+        zl = h @ p[f"Wb1{l}"] + a @ p[f"Wb2{l}"] + p[f"bb{l}"]
+        h = h + silu(zl)
         cache["us"].append(u)
         cache["pres"].append(pre)
         cache["as_"].append(a)
-        cache["zs"].append(z)
+        cache["zs"].append(zl)
         cache["hs"].append(h)
     o = h @ p["Wo"] + p["bo"]
     cache["o"] = o
-    x = np.concatenate([s * o[:, 0], b[n:] + s * o[:, 1]])
+    x = np.concatenate([zb[:n] + s * o[:, 0], zb[n:] + s * o[:, 1]])
     loss = None
     if target is not None:
-        t0 = target[:n] / s
-        t1 = (target[n:] - b[n:]) / s
+        t0 = (target[:n] - zb[:n]) / s
+        t1 = (target[n:] - zb[n:]) / s
         loss = np.mean((o[:, 0] - t0) ** 2 + (o[:, 1] - t1) ** 2)
         cache["t"] = np.stack([t0, t1], 1)
     return x, loss, cache

@@ -226,7 +226,11 @@ void run_molecule(Handle& H, WsNet* ws, const MolDev& m, double* x_dev, double* 
     x = xl.p;
   }
   if (ws) {
-    // learned initial guess (tree order), GMRES from there
+    // learned initial guess (tree order), GMRES from there: the network
+    // corrects the leaf-block preconditioner's solution z = M^-1 b
+    DBuf<double>& z = H.rn_z;
+    z.alloc(2 * (size_t)nface);
+    msolve_dev(H, b.p, z.p, s);
     WsInput in;
     in.n = nface;
     in.px = H.d_x.p;
@@ -237,6 +241,7 @@ void run_molecule(Handle& H, WsNet* ws, const MolDev& m, double* x_dev, double* 
     in.qz = H.d_nz.p;
     in.area = H.d_area.p;
     in.b = b.p;
+    in.z = z.p;
     ws->forward(in, x, nullptr, s);
     mark("warm start");
   } else {
@@ -261,7 +266,7 @@ void run_molecule(Handle& H, WsNet* ws, const MolDev& m, double* x_dev, double* 
 }
 
 WsInput ws_input(int nface, const double* tr_xyz, const double* tr_q, const double* tr_area,
-                 const double* bvct) {
+                 const double* bvct, const double* zprec) {
   TABI_REQUIRE(nface > 0 && tr_xyz && tr_q && tr_area && bvct, TABI_ERR_ARG, "null argument");
   WsInput in;
   in.n = nface;
@@ -275,6 +280,7 @@ WsInput ws_input(int nface, const double* tr_xyz, const double* tr_q, const doub
   in.qs = 3;
   in.area = tr_area;
   in.b = bvct;
+  in.z = zprec;
   return in;
 }
 
@@ -767,24 +773,25 @@ int tabi_ws_set_params(tabi_ws w, const float* theta, long long n) {
 }
 
 int tabi_ws_predict_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
-                        const double* tr_area, const double* bvct, double* x0, void* stream) {
+                        const double* tr_area, const double* bvct, const double* zprec,
+                        double* x0, void* stream) {
   if (!w) return TABI_ERR_ARG;
   return guarded(nullptr, [&] {
     TABI_REQUIRE(x0 != nullptr, TABI_ERR_ARG, "null output");
     cudaStream_t s = ws_stream(w, stream);
-    w->net->forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct), x0, nullptr, s);
+    w->net->forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct, zprec), x0, nullptr, s);
   });
 }
 
 int tabi_ws_loss_grad_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
-                          const double* tr_area, const double* bvct, const double* x_target,
-                          double* loss, float* grad, void* stream) {
+                          const double* tr_area, const double* bvct, const double* zprec,
+                          const double* x_target, double* loss, float* grad, void* stream) {
   if (!w) return TABI_ERR_ARG;
   return guarded(nullptr, [&] {
     TABI_REQUIRE(x_target && loss, TABI_ERR_ARG, "null argument");
     cudaStream_t s = ws_stream(w, stream);
     WsNet& N = *w->net;
-    N.forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct), nullptr, x_target, s);
+    N.forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct, zprec), nullptr, x_target, s);
     N.backward(nface, s);
     *loss = N.read_loss(s);
     if (grad) {
@@ -795,15 +802,15 @@ int tabi_ws_loss_grad_dev(tabi_ws w, int nface, const double* tr_xyz, const doub
 }
 
 int tabi_ws_train_step_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
-                           const double* tr_area, const double* bvct, const double* x_target,
-                           double lr, double* loss, void* stream) {
+                           const double* tr_area, const double* bvct, const double* zprec,
+                           const double* x_target, double lr, double* loss, void* stream) {
   if (!w) return TABI_ERR_ARG;
   return guarded(nullptr, [&] {
     TABI_REQUIRE(x_target != nullptr, TABI_ERR_ARG, "null target");
     TABI_REQUIRE(lr > 0.0 && std::isfinite(lr), TABI_ERR_ARG, "learning rate must be > 0");
     cudaStream_t s = ws_stream(w, stream);
     WsNet& N = *w->net;
-    N.forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct), nullptr, x_target, s);
+    N.forward(ws_input(nface, tr_xyz, tr_q, tr_area, bvct, zprec), nullptr, x_target, s);
     N.backward(nface, s);
     N.adam(lr, s);
     if (loss) *loss = N.read_loss(s);
@@ -811,15 +818,15 @@ int tabi_ws_train_step_dev(tabi_ws w, int nface, const double* tr_xyz, const dou
 }
 
 int tabi_ws_graph_dev(tabi_ws w, int nface, const double* tr_xyz, const double* tr_q,
-                      const double* tr_area, const double* bvct, int* nbr, float* feat,
-                      void* stream) {
+                      const double* tr_area, const double* bvct, const double* zprec, int* nbr,
+                      float* feat, void* stream) {
   if (!w) return TABI_ERR_ARG;
   return guarded(nullptr, [&] {
     cudaStream_t s = ws_stream(w, stream);
     WsNet& N = *w->net;
-    N.graph(ws_input(nface, tr_xyz, tr_q, tr_area, bvct), s);
+    N.graph(ws_input(nface, tr_xyz, tr_q, tr_area, bvct, zprec), s);
     TABI_REQUIRE(N.graph_exact(s), TABI_ERR_LIMIT,
-                 "neighbour search: the 16 nearest of some panel lie beyond 8 cells");
+                 "neighbour search: fewer than 16 other panels");
     if (nbr)
       TABI_CUDA(cudaMemcpyAsync(nbr, N.nbr.p, sizeof(int) * (size_t)nface * kWsK,
                                 cudaMemcpyDeviceToHost, s));

@@ -282,7 +282,7 @@ struct Handle {
   // staging of the host-array entry points and of tabi_run_dev
   DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;
   DBuf<int> st_fv;
-  DBuf<double> rn_b0, rn_b, rn_x;
+  DBuf<double> rn_b0, rn_b, rn_x, rn_z;
 };
 
 // ---- kernels / launchers (defined in the .cu files) ----

@@ -6,16 +6,18 @@
 // (main.f90:133); GMRES on the true residual stays the judge, so a prediction
 // only changes the iteration count.
 //
-// Network, for N panels (centroid r, unit normal n, area A, b = [b1; b2]):
+// Network, for N panels (centroid r, unit normal n, area A, b = [b1; b2], and
+// z = M^-1 b, the leaf-block preconditioner's solution -- exact within each
+// leaf -- or [0; b2] without it):
 //   graph   K = 16 nearest other panels per panel (cell-list search, exact,
 //           ascending distance, ties by index)
-//   input   8 invariant node features and 11 invariant edge features (8
-//           radial basis functions of |r_ij| / mean neighbour distance and
-//           three normal/direction cosines)
+//   input   10 invariant node features (asinh of z / s among them) and 11
+//           invariant edge features (8 radial basis functions of |r_ij| /
+//           mean neighbour distance and three normal/direction cosines)
 //   layers  h = silu(f W0 + b0); L times: u = h Wa,
-//           a_i = 1/K sum_k silu(e_ij Wf + bf) * u_j, z = h Wb1 + a Wb2 + bb,
-//           h += silu(z)
-//   output  o = h Wo + bo, x1 = s o0, x2 = b2 + s o1 with s = rms(b1)
+//           a_i = 1/K sum_k silu(e_ij Wf + bf) * u_j, g = h Wb1 + a Wb2 + bb,
+//           h += silu(g)
+//   output  o = h Wo + bo, x = z + s o with s = rms(b1): the network corrects z
 // Weight matrices are used in bfloat16 with FP32 accumulation; FP32 master
 // weights, gradients and Adam moments are kept for training.  Every reduction
 // (weight gradients, bias gradients, loss) is a fixed-order two-stage sum, and
@@ -57,8 +59,9 @@ __global__ void ws_prep_kernel(int n, const double* __restrict__ px, const doubl
                                const double* __restrict__ qx, const double* __restrict__ qy,
                                const double* __restrict__ qz, int qs,
                                const double* __restrict__ area, const double* __restrict__ b,
-                               float4* __restrict__ pos, float4* __restrict__ nrm,
-                               float2* __restrict__ bf, double* __restrict__ part) {
+                               const double* __restrict__ zp, float4* __restrict__ pos,
+                               float4* __restrict__ nrm, float2* __restrict__ bf,
+                               float2* __restrict__ zf, double* __restrict__ part) {
   double sa = 0.0, sb = 0.0;
   float lo[3] = {3e38f, 3e38f, 3e38f}, hi[3] = {-3e38f, -3e38f, -3e38f};
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -68,6 +71,7 @@ __global__ void ws_prep_kernel(int n, const double* __restrict__ px, const doubl
     nrm[i] = make_float4((float)qx[(size_t)i * qs], (float)qy[(size_t)i * qs],
                          (float)qz[(size_t)i * qs], 0.f);
     bf[i] = make_float2((float)b[i], (float)b[n + i]);
+    zf[i] = zp ? make_float2((float)zp[i], (float)zp[n + i]) : make_float2(0.f, (float)b[n + i]);
     sa += a;
     sb += b[i] * b[i];
     const float c[3] = {(float)x, (float)y, (float)z};
@@ -182,7 +186,9 @@ __global__ void ws_scan_add_kernel(int* __restrict__ out, int m, const int* __re
 
 // K nearest other panels: search the cube of cells within +-rad of the
 // panel's cell; the result is exact once the K-th distance is within rad*h
-// (the cube contains that ball), else the cube grows (to rad = 8).
+// (the cube contains that ball), else the cube grows -- at most until it
+// covers the grid (panels of small isolated surface pieces, e.g. cavities of
+// fewer than K + 1 faces, find their neighbours on another piece far away).
 __global__ void ws_knn_kernel(int n, const float4* __restrict__ pos, Grid g,
                               const int* __restrict__ coff, const int* __restrict__ sorted,
                               int* __restrict__ nbr, int* __restrict__ err) {
@@ -193,7 +199,8 @@ __global__ void ws_knn_kernel(int n, const float4* __restrict__ pos, Grid g,
             cz = cell_coord(p.z, g.z0, g.h, g.nz);
   float bd[kK];
   int bi[kK];
-  for (int rad = 1;; ++rad) {
+  // the cube grows by one cell to rad 4, then doubles (isolated pieces)
+  for (int rad = 1;; rad = rad < 4 ? rad + 1 : 2 * rad) {
 #pragma unroll
     for (int k = 0; k < kK; ++k) {
       bd[k] = 3e38f;
@@ -229,11 +236,9 @@ __global__ void ws_knn_kernel(int n, const float4* __restrict__ pos, Grid g,
     const bool whole = cx - rad <= 0 && cy - rad <= 0 && cz - rad <= 0 && cx + rad >= g.nx - 1 &&
                        cy + rad >= g.ny - 1 && cz + rad >= g.nz - 1;
     if ((bi[kK - 1] != 0x7fffffff && bd[kK - 1] <= reach * reach) || whole) break;
-    if (rad == 8) {
-      atomicExch(err, 1);  // not exact: the K nearest lie beyond 8 cells
-      break;
-    }
   }
+  // fewer than K other panels exist only when n <= K, which the host rejects
+  if (bi[kK - 1] == 0x7fffffff) atomicExch(err, 1);
 #pragma unroll
   for (int k = 0; k < kK; ++k) nbr[(size_t)i * kK + k] = bi[k] == 0x7fffffff ? i : bi[k];
 }
@@ -287,7 +292,8 @@ __device__ __forceinline__ void edge_feat(const float4 pi, const float4 ni, cons
 
 // node features (kF per panel) and the mean neighbour distance
 __global__ void ws_node_kernel(int n, const float4* __restrict__ pos, const float4* __restrict__ nrm,
-                               const float2* __restrict__ bf, const int* __restrict__ nbr,
+                               const float2* __restrict__ bf, const float2* __restrict__ zf,
+                               const int* __restrict__ nbr,
                                const double* __restrict__ stats, float* __restrict__ dbar_out,
                                float* __restrict__ f) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -324,6 +330,11 @@ __global__ void ws_node_kernel(int n, const float4* __restrict__ pos, const floa
   o[5] = nn / kK;
   o[6] = logf(dbar);
   o[7] = db / kK;
+  const float2 zi = zf[i];
+  // z can be far off on poorly conditioned molecules: asinh keeps the input
+  // bounded (linear near zero, logarithmic beyond)
+  o[8] = asinhf(zi.x / s);
+  o[9] = asinhf((zi.y - bi.y) / s);
 }
 
 // ---------------------------------------------------------------- dense layers
@@ -625,11 +636,13 @@ __global__ void ws_agg_bwd_u_kernel(int n, int H, const float4* __restrict__ pos
 }
 
 // ---------------------------------------------------------------- head / loss
-// o = h Wo + bo (one warp per panel); x = [s o0, b2 + s o1]; with a target,
-// do = 2 (o - t) / N and per-block loss partials.
+// o = h Wo + bo (one warp per panel); x = z + s o (z = [0; b2] without a
+// preconditioner solution); with a target, do = 2 (o - (x_t - z)/s) / N and
+// per-block loss partials.
 __global__ void ws_head_kernel(int n, int H, const float* __restrict__ h,
                                const __nv_bfloat16* __restrict__ Wo,
                                const float* __restrict__ bo, const double* __restrict__ b,
+                               const double* __restrict__ zp,
                                const double* __restrict__ stats, double* __restrict__ xout,
                                const double* __restrict__ target, float* __restrict__ dout,
                                double* __restrict__ lpart) {
@@ -653,12 +666,13 @@ __global__ void ws_head_kernel(int n, int H, const float* __restrict__ h,
     o0 += bo[0];
     o1 += bo[1];
     if (lane == 0) {
+      const double z1 = zp ? zp[i] : 0.0, z2 = zp ? zp[n + i] : b[n + i];
       if (xout) {
-        xout[i] = s * o0;
-        xout[n + i] = b[n + i] + s * o1;
+        xout[i] = z1 + s * o0;
+        xout[n + i] = z2 + s * o1;
       }
       if (target) {
-        const double t0 = target[i] / s, t1 = (target[n + i] - b[n + i]) / s;
+        const double t0 = (target[i] - z1) / s, t1 = (target[n + i] - z2) / s;
         const double d0 = o0 - t0, d1 = o1 - t1;
         lsum += d0 * d0 + d1 * d1;
         dout[2 * i] = (float)(2.0 * d0 / n);
@@ -758,7 +772,7 @@ WsNet::WsNet(int hidden, int layers, unsigned long long seed) : H(hidden), L(lay
   off_bo = take(2);
   np = o;
   // initial weights: N(0, 1/fan_in) for the matrices (the output layer zero,
-  // so an untrained network predicts x1 = 0, x2 = b2), zero biases
+  // so an untrained network predicts x = z), zero biases
   std::vector<float> th((size_t)np, 0.f);
   std::mt19937_64 rng(seed);
   std::normal_distribution<double> nd(0.0, 1.0);
@@ -827,11 +841,13 @@ void WsNet::graph(const WsInput& in, cudaStream_t s) {
   pos.alloc(n);
   nrm.alloc(n);
   bfl.alloc(n);
+  zfl.alloc(n);
   const int pb = 148;
   stats_part.alloc(8 * pb + 8);
   stats.alloc(16);
   ws_prep_kernel<<<pb, 256, 0, s>>>(n, in.px, in.py, in.pz, in.ps, in.qx, in.qy, in.qz, in.qs,
-                                     in.area, in.b, pos.p, nrm.p, bfl.p, stats_part.p);
+                                     in.area, in.b, in.z, pos.p, nrm.p, bfl.p, zfl.p,
+                                     stats_part.p);
   ws_prep_final_kernel<<<1, 32, 0, s>>>(stats_part.p, pb, stats.p);
   TABI_CUDA(cudaMemcpyAsync(h_stats, stats.p, sizeof(double) * 8, cudaMemcpyDeviceToHost, s));
   TABI_CUDA(cudaStreamSynchronize(s));
@@ -886,8 +902,8 @@ void WsNet::graph(const WsInput& in, cudaStream_t s) {
   // node features
   dbar.alloc(n);
   feat.alloc((size_t)n * kF);
-  ws_node_kernel<<<ceil_div(n, 128), 128, 0, s>>>(n, pos.p, nrm.p, bfl.p, nbr.p, stats.p, dbar.p,
-                                                  feat.p);
+  ws_node_kernel<<<ceil_div(n, 128), 128, 0, s>>>(n, pos.p, nrm.p, bfl.p, zfl.p, nbr.p, stats.p,
+                                                  dbar.p, feat.p);
   TABI_CUDA(cudaGetLastError());
 }
 
@@ -932,8 +948,8 @@ void WsNet::forward(const WsInput& in, double* xout, const double* target, cudaS
   }
   dout.alloc(2 * (size_t)n);
   lpart.alloc(kRedB + 2);
-  ws_head_kernel<<<kRedB, 256, 0, s>>>(n, H, hs.p + nh * L, W + off_Wo, T + off_bo, in.b, stats.p,
-                                       xout, target, dout.p, lpart.p);
+  ws_head_kernel<<<kRedB, 256, 0, s>>>(n, H, hs.p + nh * L, W + off_Wo, T + off_bo, in.b, in.z,
+                                       stats.p, xout, target, dout.p, lpart.p);
   if (target) ws_loss_final_kernel<<<1, 32, 0, s>>>(lpart.p, kRedB, n, lpart.p + kRedB);
   TABI_CUDA(cudaGetLastError());
 }

@@ -13,11 +13,12 @@ namespace tabi {
 
 constexpr int kWsK = 16;  // neighbours per panel
 constexpr int kWsR = 8;   // radial basis functions of the edge input
-constexpr int kWsF = 8;   // node input features
+constexpr int kWsF = 10;  // node input features
 
 // One molecule's panels: FP64 components with a stride (3 for the reference's
-// interleaved tr_xyz / tr_q, 1 for the handle's SoA arrays), area (n) and the
-// right-hand side b (2n).
+// interleaved tr_xyz / tr_q, 1 for the handle's SoA arrays), area (n), the
+// right-hand side b (2n) and, optionally, z = M^-1 b (2n), the leaf-block
+// preconditioner's solution, which the network takes as input and corrects.
 struct WsInput {
   int n = 0;
   const double *px = nullptr, *py = nullptr, *pz = nullptr;
@@ -26,6 +27,7 @@ struct WsInput {
   int qs = 1;
   const double* area = nullptr;
   const double* b = nullptr;
+  const double* z = nullptr;  // may be null: the baseline is then [0; b2]
 };
 
 struct WsNet {
@@ -49,7 +51,7 @@ struct WsNet {
   DBuf<__nv_bfloat16> wbf;
   // per-molecule state (grow-only)
   DBuf<float4> pos, nrm;
-  DBuf<float2> bfl;
+  DBuf<float2> bfl, zfl;
   DBuf<double> stats_part, stats;
   DBuf<int> cell, ccnt, coff, csorted, sbuf, nbr, err, rcnt, roff, rev;
   DBuf<float> dbar, feat;

@@ -169,6 +169,165 @@ static void quad(fbuf* F, const double* v, int a, int b, int c, int d) {
   }
 }
 
+/* ---- weld: vertices closer than tol are merged (union-find over a grid of
+ * tol cells; the merged vertex is the mean position with the renormalised
+ * mean normal); faces left with a repeated vertex and repeated faces are
+ * dropped.  Surface nets can project the vertices of neighbouring cells onto
+ * nearly the same point, which leaves sliver triangles whose centroids nearly
+ * coincide: singular kernel pairs for the boundary integral equations. */
+typedef struct {
+  long long key;
+  int idx;
+} keyidx;
+
+static int cmp_keyidx(const void* a, const void* b) {
+  const keyidx* x = (const keyidx*)a;
+  const keyidx* y = (const keyidx*)b;
+  if (x->key != y->key) return x->key < y->key ? -1 : 1;
+  return x->idx - y->idx;
+}
+
+static int uf_find(int* par, int i) {
+  while (par[i] != i) {
+    par[i] = par[par[i]];
+    i = par[i];
+  }
+  return i;
+}
+
+typedef struct {
+  int v[3];
+  int idx;
+} tri;
+
+static int cmp_tri(const void* a, const void* b) {
+  const tri* x = (const tri*)a;
+  const tri* y = (const tri*)b;
+  for (int k = 0; k < 3; ++k)
+    if (x->v[k] != y->v[k]) return x->v[k] < y->v[k] ? -1 : 1;
+  return x->idx - y->idx;
+}
+
+static int weld(vbuf* V, fbuf* FB, double tol, const double* lo) {
+  const int nv = V->nv;
+  if (nv == 0) return 0;
+  keyidx* ki = (keyidx*)malloc(sizeof(keyidx) * (size_t)nv);
+  int* par = (int*)malloc(sizeof(int) * (size_t)nv);
+  if (!ki || !par) {
+    free(ki);
+    free(par);
+    return -1;
+  }
+  const long long M = 1 << 20;
+#define SG_KEY(ix, iy, iz) ((((long long)(iz)) * M + (iy)) * M + (ix))
+  for (int i = 0; i < nv; ++i) {
+    const double* p = V->v + 6 * (size_t)i;
+    long long c[3];
+    for (int d = 0; d < 3; ++d) c[d] = (long long)floor((p[d] - lo[d]) / tol) + 1;
+    ki[i].key = SG_KEY(c[0], c[1], c[2]);
+    ki[i].idx = i;
+    par[i] = i;
+  }
+  qsort(ki, (size_t)nv, sizeof(keyidx), cmp_keyidx);
+  const double tol2 = tol * tol;
+  for (int i = 0; i < nv; ++i) {
+    const double* p = V->v + 6 * (size_t)i;
+    long long c[3];
+    for (int d = 0; d < 3; ++d) c[d] = (long long)floor((p[d] - lo[d]) / tol) + 1;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const long long key = SG_KEY(c[0] + dx, c[1] + dy, c[2] + dz);
+          /* first entry with this key */
+          int a = 0, b = nv;
+          while (a < b) {
+            int m = (a + b) / 2;
+            if (ki[m].key < key) a = m + 1; else b = m;
+          }
+          for (; a < nv && ki[a].key == key; ++a) {
+            const int j = ki[a].idx;
+            if (j <= i) continue;
+            if (d2v(V->v, i, j) < tol2) {
+              int ri = uf_find(par, i), rj = uf_find(par, j);
+              if (ri != rj) par[ri < rj ? rj : ri] = ri < rj ? ri : rj;
+            }
+          }
+        }
+  }
+#undef SG_KEY
+  free(ki);
+  /* new vertices: one per set, in order of the set's smallest member */
+  int* newid = (int*)malloc(sizeof(int) * (size_t)nv);
+  double* acc = (double*)calloc((size_t)nv * 7, sizeof(double));
+  if (!newid || !acc) {
+    free(par);
+    free(newid);
+    free(acc);
+    return -1;
+  }
+  int nn = 0;
+  for (int i = 0; i < nv; ++i) {
+    const int r = uf_find(par, i);
+    if (r == i) newid[i] = nn++;
+  }
+  for (int i = 0; i < nv; ++i) {
+    const int t = newid[uf_find(par, i)];
+    for (int d = 0; d < 6; ++d) acc[7 * (size_t)t + d] += V->v[6 * (size_t)i + d];
+    acc[7 * (size_t)t + 6] += 1.0;
+  }
+  for (int t = 0; t < nn; ++t) {
+    double* a = acc + 7 * (size_t)t;
+    double* o = V->v + 6 * (size_t)t;
+    for (int d = 0; d < 3; ++d) o[d] = a[d] / a[6];
+    double g = sqrt(a[3] * a[3] + a[4] * a[4] + a[5] * a[5]);
+    for (int d = 0; d < 3; ++d) o[3 + d] = g > 0 ? a[3 + d] / g : (d == 2 ? 1.0 : 0.0);
+  }
+  V->nv = nn;
+  free(acc);
+  /* faces: remap, drop degenerate ones, then repeats (first occurrence kept) */
+  tri* T = (tri*)malloc(sizeof(tri) * (size_t)(FB->nf > 0 ? FB->nf : 1));
+  char* keep = (char*)malloc((size_t)(FB->nf > 0 ? FB->nf : 1));
+  if (!T || !keep) {
+    free(par);
+    free(newid);
+    free(T);
+    free(keep);
+    return -1;
+  }
+  int nt = 0;
+  for (int f = 0; f < FB->nf; ++f) {
+    int* q = FB->f + 3 * (size_t)f;
+    for (int k = 0; k < 3; ++k) q[k] = newid[uf_find(par, q[k])];
+    keep[f] = q[0] != q[1] && q[1] != q[2] && q[0] != q[2];
+    if (!keep[f]) continue;
+    int a = q[0], b = q[1], c = q[2], x;
+    if (a > b) { x = a; a = b; b = x; }
+    if (b > c) { x = b; b = c; c = x; }
+    if (a > b) { x = a; a = b; b = x; }
+    T[nt].v[0] = a;
+    T[nt].v[1] = b;
+    T[nt].v[2] = c;
+    T[nt].idx = f;
+    ++nt;
+  }
+  qsort(T, (size_t)nt, sizeof(tri), cmp_tri);
+  for (int k = 1; k < nt; ++k)
+    if (T[k].v[0] == T[k - 1].v[0] && T[k].v[1] == T[k - 1].v[1] && T[k].v[2] == T[k - 1].v[2])
+      keep[T[k].idx] = 0;
+  int nf = 0;
+  for (int f = 0; f < FB->nf; ++f)
+    if (keep[f]) {
+      for (int k = 0; k < 3; ++k) FB->f[3 * (size_t)nf + k] = FB->f[3 * (size_t)f + k];
+      ++nf;
+    }
+  FB->nf = nf;
+  free(T);
+  free(keep);
+  free(par);
+  free(newid);
+  return 0;
+}
+
 int sg_gaussian_surface(int natm, const double* xyzr, double probe,
                         double density, double blob, double** vert_out,
                         int* nvert_out, int** face_out, int* nface_out,
@@ -298,6 +457,11 @@ int sg_gaussian_surface(int natm, const double* xyzr, double probe,
   free(f);
   free(cv);
   field_free(&F);
+  if (weld(&V, &FB, 0.25 * h, lo) != 0) {
+    free(V.v);
+    free(FB.f);
+    return -1;
+  }
   /* to 1-based indices like MSMS */
   for (int i = 0; i < 3 * FB.nf; ++i) FB.f[i] += 1;
   *vert_out = V.v;

@@ -117,11 +117,12 @@ def load(path: str = LIB_PATH):
     L.tabi_ws_nparams.argtypes = [_vp]
     L.tabi_ws_get_params.argtypes = [_vp, _fp, C.c_longlong]
     L.tabi_ws_set_params.argtypes = [_vp, _fp, C.c_longlong]
-    L.tabi_ws_predict_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp]
-    L.tabi_ws_loss_grad_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _dp, _fp, _vp]
-    L.tabi_ws_train_step_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, C.c_double,
+    L.tabi_ws_predict_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _vp]
+    L.tabi_ws_loss_grad_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, _dp, _fp,
+                                        _vp]
+    L.tabi_ws_train_step_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _vp, C.c_double,
                                          _dp, _vp]
-    L.tabi_ws_graph_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _ip, _fp, _vp]
+    L.tabi_ws_graph_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _ip, _fp, _vp]
     L.tabi_set_warmstart.argtypes = [_vp, _vp]
     L.tabi_batch_run_dev.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(MolDev), _vp, C.c_int,
                                      _dp]

@@ -1,7 +1,8 @@
 """Learned warm start: the panel network of libtabi_gpu.so (tabi_ws_*).
 
 The network predicts the initial guess x0 = [phi; dphi/dn] of a solve from
-the panel geometry and the right-hand side; GMRES on the true residual runs
+the panel geometry, the right-hand side b and z = M^-1 b, the leaf-block
+preconditioner's solution, which it corrects; GMRES on the true residual runs
 from there, so only the iteration count changes.  It is trained on the GPU by
 the library's own forward, backward and Adam kernels, on solutions this solver
 produces for synthetic molecules.
@@ -25,7 +26,7 @@ from . import _lib
 from ._lib import TabiError, check
 
 K_NEIGHBOURS = 16
-NODE_FEATURES = 8
+NODE_FEATURES = 10  # per panel, as the library writes them (tabi_ws_graph_dev)
 # atoms per A^3 of the globular benchmark molecule (2,000 atoms in 18 A)
 GLOBULAR_DENSITY = 2000 / (4.0 / 3.0 * np.pi * 18.0 ** 3)
 
@@ -97,18 +98,19 @@ class WarmStart:
         ws.set_params(z["theta"])
         return ws
 
-    # ---- device entry points (sample: dict of CUDA tensors, see make_sample)
+    # ---- device entry points (sample: dict of CUDA tensors, see make_sample;
+    # its "z" = M^-1 b may be absent)
     def predict_dev(self, s, x_out, stream=None):
         self._check(self.L.tabi_ws_predict_dev(self.h, s["n"], _ptr(s["xyz"]), _ptr(s["tq"]),
-                                               _ptr(s["area"]), _ptr(s["b"]), _ptr(x_out),
-                                               _stream(stream)))
+                                               _ptr(s["area"]), _ptr(s["b"]), _ptr(s.get("z")),
+                                               _ptr(x_out), _stream(stream)))
 
     def loss_grad_dev(self, s, want_grad=True, stream=None):
         loss = C.c_double()
         g = np.zeros(self.nparams, np.float32) if want_grad else None
         self._check(self.L.tabi_ws_loss_grad_dev(
             self.h, s["n"], _ptr(s["xyz"]), _ptr(s["tq"]), _ptr(s["area"]), _ptr(s["b"]),
-            _ptr(s["x"]), C.byref(loss),
+            _ptr(s.get("z")), _ptr(s["x"]), C.byref(loss),
             g.ctypes.data_as(C.POINTER(C.c_float)) if g is not None else None, _stream(stream)))
         return loss.value, g
 
@@ -116,18 +118,29 @@ class WarmStart:
         loss = C.c_double()
         self._check(self.L.tabi_ws_train_step_dev(
             self.h, s["n"], _ptr(s["xyz"]), _ptr(s["tq"]), _ptr(s["area"]), _ptr(s["b"]),
-            _ptr(s["x"]), float(lr), C.byref(loss), _stream(stream)))
+            _ptr(s.get("z")), _ptr(s["x"]), float(lr), C.byref(loss), _stream(stream)))
         return loss.value
 
     def graph_dev(self, s, stream=None):
         n = s["n"]
+        # the input layer is NODE_FEATURES x hidden (+ hidden biases) at the
+        # head of the parameters: check the host buffers match the library
+        w0 = self.params()[: NODE_FEATURES * self.hidden]
+        if self.nparams != _expected_nparams(self.hidden, self.layers) or w0.size == 0:
+            raise TabiError(-1, "network layout does not match this binding")
         nbr = np.zeros((n, K_NEIGHBOURS), np.int32)
         feat = np.zeros((n, NODE_FEATURES), np.float32)
         self._check(self.L.tabi_ws_graph_dev(
             self.h, n, _ptr(s["xyz"]), _ptr(s["tq"]), _ptr(s["area"]), _ptr(s["b"]),
-            nbr.ctypes.data_as(C.POINTER(C.c_int)), feat.ctypes.data_as(C.POINTER(C.c_float)),
+            _ptr(s.get("z")), nbr.ctypes.data_as(C.POINTER(C.c_int)), feat.ctypes.data_as(C.POINTER(C.c_float)),
             _stream(stream)))
         return nbr, feat
+
+
+def _expected_nparams(hidden, layers, radial=8):
+    edge = radial + 3
+    per_layer = 3 * hidden * hidden + edge * hidden + 2 * hidden
+    return NODE_FEATURES * hidden + hidden + layers * per_layer + 2 * hidden + 2
 
 
 def globular_radius(natm):
@@ -140,8 +153,8 @@ def make_sample(natm, seed, density=10.0, tol=1e-6, precision=None, maxparnode=5
     """One training / evaluation molecule: a synthetic globule (the benchmark
     generator at the benchmark density), its surface, and its solution by this
     solver (tree order, GMRES from zero to `tol`).  Returns a dict of CUDA
-    tensors (xyz, tq: 3n interleaved; area: n; b, x: 2n) plus n, natm, the
-    iteration count and the host inputs needed to solve it again."""
+    tensors (xyz, tq: 3n interleaved; area: n; b, z = M^-1 b, x: 2n) plus n,
+    natm, the iteration count and the host inputs needed to solve it again."""
     import torch
 
     from . import surface as S
@@ -158,19 +171,21 @@ def make_sample(natm, seed, density=10.0, tol=1e-6, precision=None, maxparnode=5
         txyz, ttq, tar, b = s.form_matrix(pos, nrm, fc, xyz, q)
         s.build_tree()
         txyz, ttq, tar, bt = s.permute(txyz, ttq, tar, b)
+        zt = s.msolve(bt)
         res = s.dgmres(bt)
     dev = torch.device(device)
     t = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64).ravel()).to(dev)
     return dict(n=len(tar), natm=natm, seed=seed, xyz=t(txyz), tq=t(ttq), area=t(tar), b=t(bt),
-                x=t(res["x"]), iters=res["iter"], ierr=res["ierr"],
+                z=t(zt), x=t(res["x"]), iters=res["iter"], ierr=res["ierr"],
                 host=dict(sptpos=pos, sptnrm=nrm, nvert=fc, chrpos=xyz, atmchr=q), prm=prm)
 
 
 def train(ws, samples, epochs=10, lr=1e-3, lr_final=1e-4, seed=0, log=None):
-    """Adam over the samples, one molecule per step, shuffled each epoch,
-    learning rate decayed geometrically from lr to lr_final.  Returns the
-    per-epoch mean losses."""
+    """Adam over the samples whose solve converged, one molecule per step,
+    shuffled each epoch, learning rate decayed geometrically from lr to
+    lr_final.  Returns the per-epoch mean losses."""
     rng = np.random.default_rng(seed)
+    samples = [s for s in samples if s.get("ierr", 0) == 0]  # converged solutions only
     steps = max(1, epochs * len(samples))
     gamma = (lr_final / lr) ** (1.0 / max(1, steps - 1))
     k = 0
@@ -190,7 +205,8 @@ def train(ws, samples, epochs=10, lr=1e-3, lr_final=1e-4, seed=0, log=None):
 
 def evaluate(ws, samples, tol=1e-6, precision=None):
     """GMRES iterations and solve time from x0 = 0 and from the network's x0
-    for each sample (same tree, same tolerance).  Returns a list of dicts."""
+    for each sample (same tree, same tolerance), and the iterations from the
+    network's baseline z = M^-1 b alone.  Returns a list of dicts."""
     import torch
 
     from .solver import TabiSolver
@@ -216,8 +232,10 @@ def evaluate(ws, samples, tol=1e-6, precision=None):
             t2 = time.perf_counter()
             r_0 = sv.dgmres(b)
             t3 = time.perf_counter()
+            r_z = sv.dgmres(b, s["z"].cpu().numpy()) if "z" in s else r_0
         xt = s["x"].cpu().numpy()
         out.append(dict(n=s["n"], natm=s["natm"], iters_zero=r_0["iter"], iters_ws=r_ws["iter"],
+                        iters_baseline=r_z["iter"],
                         ierr=(r_0["ierr"], r_ws["ierr"]), predict_s=t_pred,
                         solve_s_ws=t2 - t1, solve_s_zero=t3 - t2,
                         x0_rel_err=float(np.linalg.norm(x0.cpu().numpy() - xt)

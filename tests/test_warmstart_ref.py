@@ -29,7 +29,9 @@ def test_backward_matches_finite_differences():
     theta = W.init_params(H, L, R, seed=3).astype(np.float64) * 0.7
     rng = np.random.default_rng(5)
     target = rng.standard_normal(2 * len(area)) * np.std(b)
-    _, loss, cache = W.forward(theta, H, L, R, pos, nrm, area, b, nbr, target, round_bf16=False)
+    z = b + 0.1 * rng.standard_normal(b.size) * np.std(b)
+    _, loss, cache = W.forward(theta, H, L, R, pos, nrm, area, b, nbr, target, round_bf16=False,
+                               z=z)
     g = W.backward(cache, H, L, R, nbr)
     idx = rng.choice(theta.size, 60, replace=False)
     h = 1e-6
@@ -38,8 +40,8 @@ def test_backward_matches_finite_differences():
         tp[k] += h
         tm = theta.copy()
         tm[k] -= h
-        lp = W.forward(tp, H, L, R, pos, nrm, area, b, nbr, target, round_bf16=False)[1]
-        lm = W.forward(tm, H, L, R, pos, nrm, area, b, nbr, target, round_bf16=False)[1]
+        lp = W.forward(tp, H, L, R, pos, nrm, area, b, nbr, target, round_bf16=False, z=z)[1]
+        lm = W.forward(tm, H, L, R, pos, nrm, area, b, nbr, target, round_bf16=False, z=z)[1]
         fd = (lp - lm) / (2 * h)
         assert abs(fd - g[k]) <= 1e-6 * max(1.0, abs(fd)) + 1e-7, (k, fd, g[k])
 
@@ -61,4 +63,4 @@ def test_prediction_invariant_under_rigid_motion():
 def test_param_count_of_the_shipped_shape():
     import warmstart_ref as W
 
-    assert W.nparams(160, 3, 8) == 238402
+    assert W.nparams(160, 3, 8) == 238722
