@@ -895,8 +895,7 @@ void build_precond(Handle& H, cudaStream_t s) {
                                 cudaMemcpyHostToDevice, s));
     if (nsteps > 0) {
       size_t smem = sizeof(double) * (size_t)mmax * kSP;
-      TABI_CUDA(cudaFuncSetAttribute(lu_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)std::max<size_t>(smem, 48 * 1024)));
+      raise_smem_limit((const void*)lu_panel_kernel, std::max<size_t>(smem, 48 * 1024));
     }
     for (int st = 0; st < nsteps; ++st) {
       const int k0 = st * kBP;
@@ -991,10 +990,8 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
   size_t smem = sizeof(double) * 2 * (size_t)T.max_leaf;
   TABI_REQUIRE(smem <= 200 * 1024, TABI_ERR_LIMIT, "leaf too large for the block solve");
   if (smem > 48 * 1024) {
-    TABI_CUDA(cudaFuncSetAttribute(solve_kernel<256>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    TABI_CUDA(cudaFuncSetAttribute(solve_kernel<512>,
-                                   cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    raise_smem_limit((const void*)solve_kernel<256>, smem);
+    raise_smem_limit((const void*)solve_kernel<512>, smem);
   }
   const bool fork = T.n_solve_big > 0 && T.n_solve_small > 0 && H.side != nullptr;
   cudaStream_t s2 = fork ? H.side : s;

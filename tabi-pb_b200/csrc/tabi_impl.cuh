@@ -4,8 +4,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <map>
+#include <mutex>
 #include <stdexcept>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/tabi_gpu.h"
@@ -313,5 +316,21 @@ double dot_dev(Handle& H, const double* a, const double* b, int n, cudaStream_t 
 double nrm2_dev(Handle& H, const double* a, int n, cudaStream_t s);
 
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+// Raises a kernel's dynamic shared memory limit on the current device to at
+// least `bytes` (never lowers it).  The limit is process-wide state of the
+// kernel, so handles solving on several host threads must not set it to their
+// own molecule's need: one thread could lower it under another's launch.
+inline void raise_smem_limit(const void* func, size_t bytes) {
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, size_t> high;
+  int dev = 0;
+  TABI_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  size_t& h = high[{func, dev}];
+  if (bytes <= h) return;
+  TABI_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
+  h = bytes;
+}
 
 }  // namespace tabi
