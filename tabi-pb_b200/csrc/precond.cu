@@ -261,6 +261,7 @@ constexpr int kPT = 256;           // panel kernel threads
 constexpr int kUT = 256;           // strip / gemm kernel threads
 constexpr int kUC = 128;           // strip width
 constexpr int kGT = 64;            // gemm tile
+constexpr int kOB = 128;           // outer block: columns right of it are updated once per block
 
 // Factor columns [c0l, c0l + nb) of the panel held in P (local column c of
 // the half is P + c * mr, local row r = global row k0 + r) starting at local
@@ -457,7 +458,8 @@ __global__ void __launch_bounds__(kPT) lu_panel_kernel(const int* __restrict__ i
 
 // item = (leaf, c0, c1, mode): columns [c0, c1) of the leaf block.
 // mode 0: left of the panel, the panel's swaps; 1: right of the panel, the
-// panel's swaps then U12 = L11^{-1} A12.
+// panel's swaps then U12 = L11^{-1} A12; 3: U12 = L11^{-1} A12 only (columns
+// right of an outer block, whose swaps were applied by lu_rowswap_kernel).
 __global__ void __launch_bounds__(kUT) lu_strip_kernel(const int4* __restrict__ items, int k0,
                                                        const int2* __restrict__ leaf_rng,
                                                        const int64_t* __restrict__ blk_off,
@@ -477,6 +479,7 @@ __global__ void __launch_bounds__(kUT) lu_strip_kernel(const int4* __restrict__ 
   const int* ip = piv + 2 * lr.x;
   const int tid = threadIdx.x;
   const int ncol = c1 - c0;
+  if (mode != 3) {
   if (tid == 0) {
     int nr = 0;
     for (int j = pj0; j < nb; ++j) s_rows[nr++] = k0 + j;
@@ -514,7 +517,8 @@ __global__ void __launch_bounds__(kUT) lu_strip_kernel(const int4* __restrict__ 
     }
     __syncthreads();
   }
-  if (mode != 1) return;
+  }
+  if (mode != 1 && mode != 3) return;
   for (int q = tid; q < nb * nb; q += kUT) {
     int c = q / nb, r = q - c * nb;
     sL11[r][c] = A[(size_t)(k0 + c) * m + k0 + r];
@@ -539,8 +543,14 @@ __global__ void __launch_bounds__(kUT) lu_strip_kernel(const int4* __restrict__ 
   }
 }
 
-// item = (leaf, r0, c0): C[r0:r0+64, c0:c0+64] -= L21[r0:, k0:k0+nb] U12[k0:k0+nb, c0:]
+// item = (leaf, r0, c0, ends): C[r0:r0+64, c0:c0+64] -= L[r0:, k0:k0+kd] U[k0:k0+kd, c0:]
+// with kd = min(kdepth, m - k0) (32 inside a panel step, 128 for the update
+// right of an outer block), staged 32 deep; rows are clipped at re and columns
+// at ce, packed as ends = (re << 16) | ce (0: both m).  The C tile is read and
+// written once per launch, so a 128-deep update moves a quarter of the bytes
+// of four 32-deep ones.
 __global__ void __launch_bounds__(kUT) lu_gemm_kernel(const int4* __restrict__ items, int k0,
+                                                      int kdepth,
                                                       const int2* __restrict__ leaf_rng,
                                                       const int64_t* __restrict__ blk_off,
                                                       double* __restrict__ lu) {
@@ -549,7 +559,8 @@ __global__ void __launch_bounds__(kUT) lu_gemm_kernel(const int4* __restrict__ i
   const int4 it = items[blockIdx.x];
   const int leaf = it.x, r0 = it.y, c0 = it.z;
   const int m = 2 * leaf_rng[leaf].y;
-  const int nb = min(kBP, m - k0);
+  const int re = it.w ? min(m, it.w >> 16) : m, ce = it.w ? min(m, it.w & 0xffff) : m;
+  const int kd = min(kdepth, m - k0);
   double* A = lu + blk_off[leaf];
   const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
   // C values first (independent of the tiles)
@@ -561,45 +572,117 @@ __global__ void __launch_bounds__(kUT) lu_gemm_kernel(const int4* __restrict__ i
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
       const int r = r0 + tr + 16 * a;
-      cv[a][b] = (c < m && r < m) ? cc[r] : 0.0;
+      cv[a][b] = (c < ce && r < re) ? cc[r] : 0.0;
     }
   }
-  for (int q = tid; q < kBP * kGT; q += kUT) {
-    int k = q / kGT, rr = q - k * kGT;
-    int r = r0 + rr;
-    sL[k][rr] = (k < nb && r < m) ? A[(size_t)(k0 + k) * m + r] : 0.0;
-    int k2 = q % kBP, cc2 = q / kBP;
-    int c = c0 + cc2;
-    sU[k2][cc2] = (k2 < nb && c < m) ? A[(size_t)c * m + k0 + k2] : 0.0;
-  }
-  __syncthreads();
   double acc[4][4];
 #pragma unroll
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+  for (int kc = 0; kc < kd; kc += kBP) {
+    const int nbk = min(kBP, kd - kc), kb = k0 + kc;
+    if (kc > 0) __syncthreads();
+    for (int q = tid; q < kBP * kGT; q += kUT) {
+      int k = q / kGT, rr = q - k * kGT;
+      int r = r0 + rr;
+      sL[k][rr] = (k < nbk && r < re) ? A[(size_t)(kb + k) * m + r] : 0.0;
+      int k2 = q % kBP, cc2 = q / kBP;
+      int c = c0 + cc2;
+      sU[k2][cc2] = (k2 < nbk && c < ce) ? A[(size_t)c * m + kb + k2] : 0.0;
+    }
+    __syncthreads();
 #pragma unroll 8
-  for (int k = 0; k < kBP; ++k) {
-    double lv[4], uv[4];
+    for (int k = 0; k < kBP; ++k) {
+      double lv[4], uv[4];
 #pragma unroll
-    for (int a = 0; a < 4; ++a) lv[a] = sL[k][tr + 16 * a];
+      for (int a = 0; a < 4; ++a) lv[a] = sL[k][tr + 16 * a];
 #pragma unroll
-    for (int b = 0; b < 4; ++b) uv[b] = sU[k][tc + 16 * b];
+      for (int b = 0; b < 4; ++b) uv[b] = sU[k][tc + 16 * b];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+      for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int b = 0; b < 4; ++b) acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
+    }
   }
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
     const int c = c0 + tc + 16 * b;
-    if (c >= m) continue;
+    if (c >= ce) continue;
     double* cc = A + (size_t)c * m;
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
       const int r = r0 + tr + 16 * a;
-      if (r < m) cc[r] = cv[a][b] - acc[a][b];
+      if (r < re) cc[r] = cv[a][b] - acc[a][b];
     }
+  }
+}
+
+// Row interchanges of an outer block (pivots K0 .. K0+nb-1, in order) as one
+// gather: per leaf (one CTA), the swaps are replayed on an index array of the
+// rows K0.. in shared memory, then the rows whose content moved are listed
+// with the row their value comes from (map row of the leaf: 2 kOB rows, 2 kOB
+// sources, count; stride 4 kOB + 1 ints).
+__global__ void __launch_bounds__(256) lu_swapmap_kernel(const int* __restrict__ leaves, int K0,
+                                                         const int2* __restrict__ leaf_rng,
+                                                         const int* __restrict__ piv,
+                                                         int* __restrict__ map) {
+  __shared__ int idx[kPanelMaxM];
+  __shared__ int cnt;
+  const int leaf = leaves[blockIdx.x];
+  const int2 lr = leaf_rng[leaf];
+  const int m = 2 * lr.y, nb = min(kOB, m - K0), mr = m - K0;
+  const int* ip = piv + 2 * lr.x;
+  int* rows = map + (size_t)blockIdx.x * (4 * kOB + 1);
+  int* src = rows + 2 * kOB;
+  for (int i = threadIdx.x; i < mr; i += blockDim.x) idx[i] = K0 + i;
+  if (threadIdx.x == 0) cnt = 0;
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int j = 0; j < nb; ++j) {
+      const int p = ip[K0 + j] - 1 - K0;
+      const int t = idx[j];
+      idx[j] = idx[p];
+      idx[p] = t;
+    }
+  __syncthreads();
+  for (int i = threadIdx.x; i < mr; i += blockDim.x)
+    if (idx[i] != K0 + i) {
+      const int q = atomicAdd(&cnt, 1);  // at most 2 nb rows move
+      rows[q] = K0 + i;
+      src[q] = idx[i];
+    }
+  __syncthreads();
+  if (threadIdx.x == 0) rows[4 * kOB] = cnt;
+}
+
+// item = (slot, c0, c1, leaf): the outer block's row interchanges on columns
+// [c0, c1), through the map of lu_swapmap_kernel (slot = the leaf's map row)
+constexpr int kRC = 16;  // columns per pass
+__global__ void __launch_bounds__(kUT) lu_rowswap_kernel(const int4* __restrict__ items,
+                                                         const int2* __restrict__ leaf_rng,
+                                                         const int64_t* __restrict__ blk_off,
+                                                         const int* __restrict__ map,
+                                                         double* __restrict__ lu) {
+  __shared__ double sV[2 * kOB][kRC];
+  const int4 it = items[blockIdx.x];
+  const int* rows = map + (size_t)it.x * (4 * kOB + 1);
+  const int* src = rows + 2 * kOB;
+  const int nr = rows[4 * kOB];
+  const int m = 2 * leaf_rng[it.w].y;
+  double* A = lu + blk_off[it.w];
+  for (int cs = it.y; cs < it.z; cs += kRC) {
+    const int nc = min(kRC, it.z - cs);
+    for (int q = threadIdx.x; q < nr * nc; q += kUT) {
+      const int row = q / nc, c = q - row * nc;
+      sV[row][c] = A[(size_t)(cs + c) * m + src[row]];
+    }
+    __syncthreads();
+    for (int q = threadIdx.x; q < nr * nc; q += kUT) {
+      const int row = q / nc, c = q - row * nc;
+      A[(size_t)(cs + c) * m + rows[row]] = sV[row][c];
+    }
+    __syncthreads();
   }
 }
 
@@ -685,12 +768,16 @@ __device__ __forceinline__ void prefetch_l2(const double* p, int ndouble) {
 }
 
 // Forward/back substitution with the factored block (DGETRS 'N') in 32-row
-// steps: gather through the pivot permutation, then per step the diagonal
-// block is applied as a 32 x 32 GEMV with its precomputed inverse (one warp)
-// and the rows below (above) are updated with a 32-wide GEMV by all threads.
-// The steps form a dependent chain, so each one's column panel and inverse
-// block are prefetched into L2 kPF steps ahead (by warp 1).  Large blocks run
-// with 512 threads; leaf_list selects the launch's leaves.
+// steps: gather through the pivot permutation, then per step every warp
+// applies the diagonal block's precomputed inverse to the step's 32 running
+// values (a 32 x 32 GEMV, redundant per warp, so no warp waits for another)
+// and updates its rows below (above) with a 32-wide GEMV.  The finalised
+// values go to a second array, so one barrier per step suffices: running
+// values r (xs in the forward sweep, fin in the backward one) and results are
+// never the same words within a step.  The steps form a dependent chain, so
+// each one's column panel and inverse block are prefetched into L2 kPF steps
+// ahead (by warp 1).  Large blocks run with 512 threads; leaf_list selects the
+// launch's leaves.  Shared memory: 2 m + NT doubles.
 template <int NT>
 __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     const int2* __restrict__ leaf_rng, const int64_t* __restrict__ blk_off,
@@ -698,14 +785,18 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     const double* __restrict__ lu, const double* __restrict__ dinv,
     const int* __restrict__ perm, int N, const double* __restrict__ r,
     double* __restrict__ z) {
-  extern __shared__ double xs[];
+  extern __shared__ double sm[];
   int leaf = leaf_list[blockIdx.x];
   int2 lr = leaf_rng[leaf];
   const int n = lr.y, m = 2 * n, ib = lr.x;
+  double* xs = sm;             // forward sweep: running; backward: results
+  double* fin = sm + m;        // forward sweep: results; backward: running
+  double* ys = sm + 2 * m;     // per warp: the step's 32 diagonal results
   const double* A = lu + blk_off[leaf];
   const double* Di = dinv + dinv_off[leaf];
   const int* pm = perm + 2 * ib;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double* yw = ys + 32 * warp;
   for (int i = tid; i < m; i += NT) {
     int src = pm[i];
     xs[i] = (src < n) ? r[ib + src] : r[N + ib + src - n];
@@ -724,40 +815,43 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     if (kp + lane < m) prefetch_l2(A + (size_t)(kp + lane) * m, kp);
     if (lane == 0) prefetch_l2(Di + (size_t)bp * 2 * kDB * kDB + kDB * kDB, kDB * kDB);
   };
-  if (warp == 1)
-    for (int q = 0; q < kPF; ++q) pf_lower(q * kDB);
-  __syncthreads();
-  // L y = P r
-  for (int k0 = 0; k0 < m; k0 += kDB) {
-    const int nb = min(kDB, m - k0);
-    if (warp == 1) pf_lower(k0 + kPF * kDB);
-    if (warp == 0) {
-      const double* Li = Di + (size_t)(k0 / kDB) * 2 * kDB * kDB;
-      double v = 0.0;
+  // step: y = Dinv * run[k0 .. k0+nb) (all warps), res[k0 ..] = y (warp 0),
+  // run[i] -= A[i, k0 .. k0+nb) y for the rows [i0, i1)
+  auto step = [&](int k0, int nb, const double* Dblk, double* run, double* res, int i0,
+                  int i1) {
+    double v = 0.0;
 #pragma unroll
-      for (int q = 0; q < kDB; ++q)
-        if (q < nb) v = fma(Li[(size_t)q * kDB + lane], xs[k0 + q], v);
-      __syncwarp();
-      if (lane < nb) xs[k0 + lane] = v;
-    }
-    __syncthreads();
-    for (int i = k0 + nb + tid; i < m; i += NT) {
+    for (int q = 0; q < kDB; ++q)
+      if (q < nb) v = fma(Dblk[(size_t)q * kDB + lane], run[k0 + q], v);
+    yw[lane] = v;
+    if (warp == 0 && lane < nb) res[k0 + lane] = v;
+    __syncwarp();
+    for (int i = i0 + tid; i < i1; i += NT) {
       const double* a = A + (size_t)k0 * m + i;
-      double s = xs[i];
+      double s = run[i];
       if (nb == kDB) {
         double t[kDB];
 #pragma unroll
         for (int q = 0; q < kDB; ++q) t[q] = a[(size_t)q * m];
 #pragma unroll
-        for (int q = 0; q < kDB; ++q) s = fma(-t[q], xs[k0 + q], s);
+        for (int q = 0; q < kDB; ++q) s = fma(-t[q], yw[q], s);
       } else {
-        for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], xs[k0 + q], s);
+        for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], yw[q], s);
       }
-      xs[i] = s;
+      run[i] = s;
     }
     __syncthreads();
+  };
+  if (warp == 1)
+    for (int q = 0; q < kPF; ++q) pf_lower(q * kDB);
+  __syncthreads();
+  // L y = P r: running values in xs, y in fin
+  for (int k0 = 0; k0 < m; k0 += kDB) {
+    const int nb = min(kDB, m - k0);
+    if (warp == 1) pf_lower(k0 + kPF * kDB);
+    step(k0, nb, Di + (size_t)(k0 / kDB) * 2 * kDB * kDB, xs, fin, k0 + nb, m);
   }
-  // U x = y
+  // U x = y: running values in fin, x in xs
   const int nblk = (m + kDB - 1) / kDB;
   if (warp == 1)
     for (int q = 0; q < kPF; ++q) pf_upper(nblk - 1 - q);
@@ -765,31 +859,7 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     const int k0 = b * kDB;
     const int nb = min(kDB, m - k0);
     if (warp == 1) pf_upper(b - kPF);
-    if (warp == 0) {
-      const double* Ui = Di + (size_t)b * 2 * kDB * kDB + kDB * kDB;
-      double v = 0.0;
-#pragma unroll
-      for (int q = 0; q < kDB; ++q)
-        if (q < nb) v = fma(Ui[(size_t)q * kDB + lane], xs[k0 + q], v);
-      __syncwarp();
-      if (lane < nb) xs[k0 + lane] = v;
-    }
-    __syncthreads();
-    for (int i = tid; i < k0; i += NT) {
-      const double* a = A + (size_t)k0 * m + i;
-      double s = xs[i];
-      if (nb == kDB) {
-        double t[kDB];
-#pragma unroll
-        for (int q = 0; q < kDB; ++q) t[q] = a[(size_t)q * m];
-#pragma unroll
-        for (int q = 0; q < kDB; ++q) s = fma(-t[q], xs[k0 + q], s);
-      } else {
-        for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], xs[k0 + q], s);
-      }
-      xs[i] = s;
-    }
-    __syncthreads();
+    step(k0, nb, Di + (size_t)b * 2 * kDB * kDB + kDB * kDB, fin, xs, 0, k0);
   }
   for (int i = tid; i < n; i += NT) {
     z[ib + i] = xs[i];
@@ -857,67 +927,134 @@ void build_precond(Handle& H, cudaStream_t s) {
     std::vector<int> order(nl);
     for (int l = 0; l < nl; ++l) order[l] = l;
     std::sort(order.begin(), order.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
-    std::vector<int> pitems;
-    std::vector<int4> sitems, gitems;
-    std::vector<int> poff(nsteps + 1), soff(nsteps + 1), goff(nsteps + 1);
-    for (int st = 0; st < nsteps; ++st) {
-      const int k0 = st * kBP;
-      poff[st] = (int)pitems.size();
-      soff[st] = (int)sitems.size();
-      goff[st] = (int)gitems.size();
+    // Two-level right-looking LU (LAPACK DGETRF order).  Outer blocks of kOB
+    // columns; inside one, 32-column panel steps update only the block's own
+    // columns (and swap the columns left of the panel).  After the block its
+    // kOB row interchanges are applied at once to the columns right of it,
+    // U12 follows by four 32-row TRSM + small GEMM steps, and the trailing
+    // matrix gets one kOB-deep update.
+    struct Launch {
+      int kind;  // 0 panel, 1 strip, 2 gemm, 3 swap map, 4 row swap
+      int k0, kdepth, off, cnt;
+    };
+    std::vector<Launch> plan;
+    std::vector<int> pitems, mleaves;
+    std::vector<int4> sitems, gitems, ritems;
+    auto emit = [&](int kind, int k0, int kdepth, size_t before, size_t after) {
+      if (after > before) plan.push_back({kind, k0, kdepth, (int)before, (int)(after - before)});
+    };
+    const auto pack = [](int re, int ce) { return (re << 16) | ce; };
+    for (int K0 = 0; K0 < mmax; K0 += kOB) {
+      for (int k0 = K0; k0 < std::min(mmax, K0 + kOB); k0 += kBP) {
+        size_t p0 = pitems.size(), s0 = sitems.size(), g0 = gitems.size();
+        for (int l : order) {
+          const int m = 2 * rng[l].y;
+          if (m > kPanelMaxM || m <= k0) continue;
+          pitems.push_back(l);
+          const int nb = std::min(kBP, m - k0), ce = std::min(m, K0 + kOB);
+          for (int c0 = 0; c0 < k0; c0 += kUC)
+            sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, k0), 0));
+          for (int c0 = k0 + nb; c0 < ce; c0 += kUC)
+            sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, ce), 1));
+          for (int r0 = k0 + nb; r0 < m; r0 += kGT)
+            for (int c0 = k0 + nb; c0 < ce; c0 += kGT)
+              gitems.push_back(make_int4(l, r0, c0, pack(m, ce)));
+        }
+        emit(0, k0, 0, p0, pitems.size());
+        emit(1, k0, 0, s0, sitems.size());
+        emit(2, k0, kBP, g0, gitems.size());
+      }
+      // the columns right of the outer block
+      const int Kend = K0 + kOB;
+      size_t m0 = mleaves.size(), r0i = ritems.size();
       for (int l : order) {
         const int m = 2 * rng[l].y;
-        if (m > kPanelMaxM || m <= k0) continue;
-        pitems.push_back(l);
-        const int nb = std::min(kBP, m - k0);
-        for (int c0 = 0; c0 < k0; c0 += kUC)
-          sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, k0), 0));
-        for (int c0 = k0 + nb; c0 < m; c0 += kUC)
-          sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, m), 1));
-        for (int r0 = k0 + nb; r0 < m; r0 += kGT)
-          for (int c0 = k0 + nb; c0 < m; c0 += kGT) gitems.push_back(make_int4(l, r0, c0, 0));
+        if (m > kPanelMaxM || m <= Kend) continue;
+        const int slot = (int)(mleaves.size() - m0);
+        mleaves.push_back(l);
+        for (int c0 = Kend; c0 < m; c0 += kUC)
+          ritems.push_back(make_int4(slot, c0, std::min(c0 + kUC, m), l));
       }
+      if (mleaves.size() == m0) continue;
+      emit(3, K0, 0, m0, mleaves.size());
+      emit(4, K0, 0, r0i, ritems.size());
+      for (int kb = K0; kb < Kend; kb += kBP) {
+        size_t s0 = sitems.size(), g0 = gitems.size();
+        for (int l : order) {
+          const int m = 2 * rng[l].y;
+          if (m > kPanelMaxM || m <= Kend) continue;
+          for (int c0 = Kend; c0 < m; c0 += kUC)
+            sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, m), 3));
+          for (int rr = kb + kBP; rr < Kend; rr += kGT)
+            for (int c0 = Kend; c0 < m; c0 += kGT)
+              gitems.push_back(make_int4(l, rr, c0, pack(Kend, m)));
+        }
+        emit(1, kb, 0, s0, sitems.size());
+        emit(2, kb, kBP, g0, gitems.size());
+      }
+      size_t g0 = gitems.size();
+      for (int l : order) {
+        const int m = 2 * rng[l].y;
+        if (m > kPanelMaxM || m <= Kend) continue;
+        for (int rr = Kend; rr < m; rr += kGT)
+          for (int c0 = Kend; c0 < m; c0 += kGT) gitems.push_back(make_int4(l, rr, c0, 0));
+      }
+      emit(2, K0, kOB, g0, gitems.size());
     }
-    poff[nsteps] = (int)pitems.size();
-    soff[nsteps] = (int)sitems.size();
-    goff[nsteps] = (int)gitems.size();
-    H.pc_list.alloc(std::max<size_t>(pitems.size(), 1));
-    H.pc_items.alloc(std::max<size_t>(sitems.size(), 1));
-    H.pc_gitems.alloc(std::max<size_t>(gitems.size(), 1));
-    if (!pitems.empty())
-      TABI_CUDA(cudaMemcpyAsync(H.pc_list.p, pitems.data(), sizeof(int) * pitems.size(),
-                                cudaMemcpyHostToDevice, s));
-    if (!sitems.empty())
-      TABI_CUDA(cudaMemcpyAsync(H.pc_items.p, sitems.data(), sizeof(int4) * sitems.size(),
-                                cudaMemcpyHostToDevice, s));
-    if (!gitems.empty())
-      TABI_CUDA(cudaMemcpyAsync(H.pc_gitems.p, gitems.data(), sizeof(int4) * gitems.size(),
-                                cudaMemcpyHostToDevice, s));
+    auto up = [&](auto& buf, const auto& v) {
+      buf.alloc(std::max<size_t>(v.size(), 1));
+      if (!v.empty())
+        TABI_CUDA(cudaMemcpyAsync(buf.p, v.data(), sizeof(v[0]) * v.size(),
+                                  cudaMemcpyHostToDevice, s));
+    };
+    up(H.pc_list, pitems);
+    up(H.pc_items, sitems);
+    up(H.pc_gitems, gitems);
+    up(H.pc_mleaves, mleaves);
+    up(H.pc_ritems, ritems);
+    size_t maxm = 1;
+    for (const Launch& L : plan)
+      if (L.kind == 3) maxm = std::max<size_t>(maxm, (size_t)L.cnt);
+    H.pc_map.alloc(maxm * (4 * kOB + 1));
     if (nsteps > 0) {
       size_t smem = sizeof(double) * (size_t)mmax * kSP;
       raise_smem_limit((const void*)lu_panel_kernel, std::max<size_t>(smem, 48 * 1024));
     }
-    for (int st = 0; st < nsteps; ++st) {
-      const int k0 = st * kBP;
-      const int np = poff[st + 1] - poff[st], ns = soff[st + 1] - soff[st],
-                ng = goff[st + 1] - goff[st];
-      if (np > 0) {
-        // shared memory for the largest block still active at this step
-        const int mr = 2 * rng[pitems[poff[st]]].y - k0;
-        TABI_K(K_LU, s);
-        lu_panel_kernel<<<np, kPT, sizeof(double) * (size_t)mr * kSP, s>>>(
-            H.pc_list.p + poff[st], k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
-            d_info.p);
-      }
-      if (ns > 0) {
-        TABI_K(K_LU_UPDATE, s);
-        lu_strip_kernel<<<ns, kUT, 0, s>>>(H.pc_items.p + soff[st], k0, T.d_leaf_rng.p,
-                                           T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
-      }
-      if (ng > 0) {
-        TABI_K(K_LU_UPDATE, s);
-        lu_gemm_kernel<<<ng, kUT, 0, s>>>(H.pc_gitems.p + goff[st], k0, T.d_leaf_rng.p,
-                                          T.d_blk_off.p, T.d_lu.p);
+    for (const Launch& L : plan) {
+      switch (L.kind) {
+        case 0: {
+          // shared memory for the largest block still active at this step
+          const int mr = 2 * rng[pitems[L.off]].y - L.k0;
+          TABI_K(K_LU, s);
+          lu_panel_kernel<<<L.cnt, kPT, sizeof(double) * (size_t)mr * kSP, s>>>(
+              H.pc_list.p + L.off, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
+              d_info.p);
+          break;
+        }
+        case 1: {
+          TABI_K(K_LU_UPDATE, s);
+          lu_strip_kernel<<<L.cnt, kUT, 0, s>>>(H.pc_items.p + L.off, L.k0, T.d_leaf_rng.p,
+                                                T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
+          break;
+        }
+        case 2: {
+          TABI_K(K_LU_UPDATE, s);
+          lu_gemm_kernel<<<L.cnt, kUT, 0, s>>>(H.pc_gitems.p + L.off, L.k0, L.kdepth,
+                                               T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p);
+          break;
+        }
+        case 3: {
+          TABI_K(K_LU_UPDATE, s);
+          lu_swapmap_kernel<<<L.cnt, 256, 0, s>>>(H.pc_mleaves.p + L.off, L.k0, T.d_leaf_rng.p,
+                                                  T.d_piv.p, H.pc_map.p);
+          break;
+        }
+        case 4: {
+          TABI_K(K_LU_UPDATE, s);
+          lu_rowswap_kernel<<<L.cnt, kUT, 0, s>>>(H.pc_ritems.p + L.off, T.d_leaf_rng.p,
+                                                  T.d_blk_off.p, H.pc_map.p, T.d_lu.p);
+          break;
+        }
       }
     }
     if (any_big) {
@@ -987,7 +1124,8 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
     TABI_CUDA(cudaGetLastError());
     return;
   }
-  size_t smem = sizeof(double) * 2 * (size_t)T.max_leaf;
+  // two arrays of the block order m = 2 * leaf size, plus 32 doubles per warp
+  size_t smem = sizeof(double) * (4 * (size_t)T.max_leaf + 512);
   TABI_REQUIRE(smem <= 200 * 1024, TABI_ERR_LIMIT, "leaf too large for the block solve");
   if (smem > 48 * 1024) {
     raise_smem_limit((const void*)solve_kernel<256>, smem);

@@ -279,8 +279,8 @@ struct Handle {
   DBuf<int> ls_tgt, ls_far, ls_near;
   DBuf<int64_t> ls_bsum, ls_foff, ls_noff;
   DBuf<int2> pc_tiles;
-  DBuf<int> pc_info, pc_list;
-  DBuf<int4> pc_items, pc_gitems;
+  DBuf<int> pc_info, pc_list, pc_mleaves, pc_map;
+  DBuf<int4> pc_items, pc_gitems, pc_ritems;
   DBuf<int2> pc_dblocks;
   // staging of the host-array entry points and of tabi_run_dev
   DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;
