@@ -466,57 +466,55 @@ __global__ void __launch_bounds__(kUT) lu_strip_kernel(const int4* __restrict__ 
                                                        double* __restrict__ lu,
                                                        const int* __restrict__ piv) {
   __shared__ double sL11[kBP][kBP + 1];
-  __shared__ double sV[2 * kBP][kUC / 2];
+  __shared__ double sV[2 * kBP][kUC / 4];
   __shared__ int s_rows[2 * kBP], s_src[2 * kBP];
+  __shared__ int s_idx[kPanelMaxM];
   __shared__ int s_nr;
   const int4 it = items[blockIdx.x];
   const int leaf = it.x, c0 = it.y, c1 = it.z, mode = it.w;
   const int2 lr = leaf_rng[leaf];
   const int m = 2 * lr.y;
   const int nb = min(kBP, m - k0);
-  const int pj0 = 0;
   double* A = lu + blk_off[leaf];
   const int* ip = piv + 2 * lr.x;
   const int tid = threadIdx.x;
   const int ncol = c1 - c0;
   if (mode != 3) {
-  if (tid == 0) {
-    int nr = 0;
-    for (int j = pj0; j < nb; ++j) s_rows[nr++] = k0 + j;
-    for (int j = pj0; j < nb; ++j) {
-      int p = ip[k0 + j] - 1;
-      bool have = false;
-      for (int q = 0; q < nr; ++q) have |= (s_rows[q] == p);
-      if (!have) s_rows[nr++] = p;
-    }
-    for (int q = 0; q < nr; ++q) s_src[q] = s_rows[q];
-    for (int j = pj0; j < nb; ++j) {  // content of the rows after each swap, in order
-      int p = ip[k0 + j] - 1, a = -1, b = -1;
-      for (int q = 0; q < nr; ++q) {
-        if (s_rows[q] == k0 + j) a = q;
-        if (s_rows[q] == p) b = q;
+    // the panel's swaps replayed on the row indices k0..m-1, then the rows
+    // whose content moved listed with the row their value comes from
+    const int mr = m - k0;
+    for (int i = tid; i < mr; i += kUT) s_idx[i] = k0 + i;
+    if (tid == 0) s_nr = 0;
+    __syncthreads();
+    if (tid == 0)
+      for (int j = 0; j < nb; ++j) {
+        const int p = ip[k0 + j] - 1 - k0;
+        const int t = s_idx[j];
+        s_idx[j] = s_idx[p];
+        s_idx[p] = t;
       }
-      int t = s_src[a];
-      s_src[a] = s_src[b];
-      s_src[b] = t;
-    }
-    s_nr = nr;
-  }
-  __syncthreads();
-  const int nr = s_nr;
-  for (int cs = 0; cs < ncol; cs += kUC / 2) {
-    const int nc = min(kUC / 2, ncol - cs);
-    for (int q = tid; q < nr * nc; q += kUT) {
-      int row = q / nc, c = q - row * nc;
-      sV[row][c] = A[(size_t)(c0 + cs + c) * m + s_src[row]];
-    }
     __syncthreads();
-    for (int q = tid; q < nr * nc; q += kUT) {
-      int row = q / nc, c = q - row * nc;
-      A[(size_t)(c0 + cs + c) * m + s_rows[row]] = sV[row][c];
-    }
+    for (int i = tid; i < mr; i += kUT)
+      if (s_idx[i] != k0 + i) {
+        const int q = atomicAdd(&s_nr, 1);  // at most 2 nb rows move
+        s_rows[q] = k0 + i;
+        s_src[q] = s_idx[i];
+      }
     __syncthreads();
-  }
+    const int nr = s_nr;
+    for (int cs = 0; cs < ncol; cs += kUC / 4) {
+      const int nc = min(kUC / 4, ncol - cs);
+      for (int q = tid; q < nr * nc; q += kUT) {
+        int row = q / nc, c = q - row * nc;
+        sV[row][c] = A[(size_t)(c0 + cs + c) * m + s_src[row]];
+      }
+      __syncthreads();
+      for (int q = tid; q < nr * nc; q += kUT) {
+        int row = q / nc, c = q - row * nc;
+        A[(size_t)(c0 + cs + c) * m + s_rows[row]] = sV[row][c];
+      }
+      __syncthreads();
+    }
   }
   if (mode != 1 && mode != 3) return;
   for (int q = tid; q < nb * nb; q += kUT) {
@@ -952,7 +950,9 @@ void build_precond(Handle& H, cudaStream_t s) {
           if (m > kPanelMaxM || m <= k0) continue;
           pitems.push_back(l);
           const int nb = std::min(kBP, m - k0), ce = std::min(m, K0 + kOB);
-          for (int c0 = 0; c0 < k0; c0 += kUC)
+          // left of the panel inside the outer block (the columns left of
+          // the block get the block's swaps at its end)
+          for (int c0 = K0; c0 < k0; c0 += kUC)
             sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, k0), 0));
           for (int c0 = k0 + nb; c0 < ce; c0 += kUC)
             sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, ce), 1));
@@ -964,18 +964,19 @@ void build_precond(Handle& H, cudaStream_t s) {
         emit(1, k0, 0, s0, sitems.size());
         emit(2, k0, kBP, g0, gitems.size());
       }
-      // the columns right of the outer block
+      // the block's row interchanges on the columns left of it and right of it
       const int Kend = K0 + kOB;
       size_t m0 = mleaves.size(), r0i = ritems.size();
       for (int l : order) {
         const int m = 2 * rng[l].y;
-        if (m > kPanelMaxM || m <= Kend) continue;
+        if (m > kPanelMaxM || m <= K0 || (K0 == 0 && m <= Kend)) continue;
         const int slot = (int)(mleaves.size() - m0);
         mleaves.push_back(l);
+        for (int c0 = 0; c0 < K0; c0 += kUC)
+          ritems.push_back(make_int4(slot, c0, std::min(c0 + kUC, K0), l));
         for (int c0 = Kend; c0 < m; c0 += kUC)
           ritems.push_back(make_int4(slot, c0, std::min(c0 + kUC, m), l));
       }
-      if (mleaves.size() == m0) continue;
       emit(3, K0, 0, m0, mleaves.size());
       emit(4, K0, 0, r0i, ritems.size());
       for (int kb = K0; kb < Kend; kb += kBP) {
@@ -1032,7 +1033,7 @@ void build_precond(Handle& H, cudaStream_t s) {
           break;
         }
         case 1: {
-          TABI_K(K_LU_UPDATE, s);
+          TABI_K(K_LU_STRIP, s);
           lu_strip_kernel<<<L.cnt, kUT, 0, s>>>(H.pc_items.p + L.off, L.k0, T.d_leaf_rng.p,
                                                 T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
           break;
@@ -1044,13 +1045,13 @@ void build_precond(Handle& H, cudaStream_t s) {
           break;
         }
         case 3: {
-          TABI_K(K_LU_UPDATE, s);
+          TABI_K(K_LU_SWAP, s);
           lu_swapmap_kernel<<<L.cnt, 256, 0, s>>>(H.pc_mleaves.p + L.off, L.k0, T.d_leaf_rng.p,
                                                   T.d_piv.p, H.pc_map.p);
           break;
         }
         case 4: {
-          TABI_K(K_LU_UPDATE, s);
+          TABI_K(K_LU_SWAP, s);
           lu_rowswap_kernel<<<L.cnt, kUT, 0, s>>>(H.pc_ritems.p + L.off, T.d_leaf_rng.p,
                                                   T.d_blk_off.p, H.pc_map.p, T.d_lu.p);
           break;

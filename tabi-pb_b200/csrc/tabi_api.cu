@@ -697,7 +697,8 @@ const char* tabi_profile_class_name(int kclass) {
   static const char* names[K_NCLASS] = {"form_matrix", "tree",   "lists",     "moments",
                                         "far",         "near",   "reduce",    "assemble",
                                         "lu_panel",    "solve",  "vector",    "energy",
-                                        "lu_update",   "lu_post",   "matvec"};
+                                        "lu_update",   "lu_post",   "lu_strip",
+                                        "lu_swap",     "matvec"};
   return (kclass >= 0 && kclass < K_NCLASS) ? names[kclass] : "all";
 }
 

@@ -152,7 +152,7 @@ struct Tree {
 // Kernel classes for the launch counters / event timers (tabi_profile_*).
 enum KClass {
   K_FORM = 0, K_TREE, K_LISTS, K_MOMENTS, K_FAR, K_NEAR, K_REDUCE, K_ASSEMBLE, K_LU,
-  K_SOLVE, K_VEC, K_ENERGY, K_LU_UPDATE, K_LU_POST,
+  K_SOLVE, K_VEC, K_ENERGY, K_LU_UPDATE, K_LU_POST, K_LU_STRIP, K_LU_SWAP,
   K_PHASE_MATVEC,  // whole treecode matvec (a phase: timed, not a launch)
   K_NCLASS
 };
