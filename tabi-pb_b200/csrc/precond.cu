@@ -262,6 +262,7 @@ constexpr int kUT = 256;           // strip / gemm kernel threads
 constexpr int kUC = 128;           // strip width
 constexpr int kGT = 64;            // gemm tile
 constexpr int kOB = 128;           // outer block: columns right of it are updated once per block
+constexpr int kPanelSmall = 320;   // rows left: panels up to this run in their own launch
 
 // Factor columns [c0l, c0l + nb) of the panel held in P (local column c of
 // the half is P + c * mr, local row r = global row k0 + r) starting at local
@@ -1024,12 +1025,35 @@ void build_precond(Handle& H, cudaStream_t s) {
     for (const Launch& L : plan) {
       switch (L.kind) {
         case 0: {
-          // shared memory for the largest block still active at this step
-          const int mr = 2 * rng[pitems[L.off]].y - L.k0;
-          TABI_K(K_LU, s);
-          lu_panel_kernel<<<L.cnt, kPT, sizeof(double) * (size_t)mr * kSP, s>>>(
-              H.pc_list.p + L.off, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
-              d_info.p);
+          // items are largest first; shared memory is sized by a launch's
+          // largest block, so blocks with at most kPanelSmall rows left run in
+          // a second launch (several CTAs per SM) on the side stream
+          int nbig = 0;
+          while (nbig < L.cnt && 2 * rng[pitems[L.off + nbig]].y - L.k0 > kPanelSmall) ++nbig;
+          const bool fork = nbig > 0 && nbig < L.cnt && H.side != nullptr;
+          if (fork) {
+            TABI_CUDA(cudaEventRecord(H.ev_fork, s));
+            TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
+          }
+          if (nbig > 0) {
+            const int mr = 2 * rng[pitems[L.off]].y - L.k0;
+            TABI_K(K_LU, s);
+            lu_panel_kernel<<<nbig, kPT, sizeof(double) * (size_t)mr * kSP, s>>>(
+                H.pc_list.p + L.off, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
+                d_info.p);
+          }
+          if (nbig < L.cnt) {
+            cudaStream_t s2 = fork ? H.side : s;
+            const int mr = 2 * rng[pitems[L.off + nbig]].y - L.k0;
+            TABI_K(K_LU, s2);
+            lu_panel_kernel<<<L.cnt - nbig, kPT, sizeof(double) * (size_t)mr * kSP, s2>>>(
+                H.pc_list.p + L.off + nbig, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p,
+                T.d_piv.p, d_info.p);
+          }
+          if (fork) {
+            TABI_CUDA(cudaEventRecord(H.ev_join, H.side));
+            TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
+          }
           break;
         }
         case 1: {
