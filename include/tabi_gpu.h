@@ -210,6 +210,22 @@ const char* tabi_profile_class_name(int kclass);
  * returns the achieved FP64 FLOP/s (2 per FMA). */
 int tabi_probe_fp64_peak(double ms, double* flops);
 
+/* main.f90:226-326 output_potential, after tabi_build_tree: x (2 nface) is
+ * the solution in tree order as tabi_solve returns it; x_orig receives it in
+ * the original face order and vert_ptl (2 per vertex: potential, normal
+ * derivative) the inverse-distance weighted average over the faces that use
+ * each vertex (at most 14, the first in face order, as the reference's
+ * 15-row table), both scaled by 332.0716 * 4 pi.  sptpos 3 x nspt, nvert
+ * 3 x nface 1-based (the faces given to tabi_form_matrix).  A vertex that no
+ * face uses gets 0/0 (NaN), as in the reference.  The writer of
+ * surface_potential.dat stays with the caller (main.f90:307-318). */
+int tabi_output_potential(tabi_h h, int nspt, const double* sptpos, int nface,
+                          const int* nvert, const double* x, double* x_orig,
+                          double* vert_ptl);
+int tabi_output_potential_dev(tabi_h h, int nspt, const double* sptpos_dev, int nface,
+                              const int* nvert_dev, const double* x_dev, double* x_orig_dev,
+                              double* vert_ptl_dev, void* stream);
+
 /* ---- Learned warm start (no counterpart in the reference, which starts
  * GMRES from zero, main.f90:133).  A rotation- and translation-invariant
  * point-cloud network over the panels (16 nearest neighbours per panel,

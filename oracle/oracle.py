@@ -78,6 +78,8 @@ def lib():
         L.or_energy.argtypes = [C.c_void_p, C.c_int, _dp, _dp, C.c_double, C.c_double,
                                 C.c_double, _dp, C.POINTER(C.c_double), C.POINTER(C.c_double),
                                 C.c_int]
+        L.or_output_potential.argtypes = [C.c_int, _dp, C.c_int, _ip, _dp, _dp, _dp, _dp]
+        L.or_output_potential.restype = None
         L.or_energy_surface.argtypes = [C.c_int, _dp, _dp, _dp, C.c_int, _dp, _dp, C.c_double,
                                         C.c_double, C.c_double, _dp, C.POINTER(C.c_double),
                                         C.POINTER(C.c_double), C.c_int]
@@ -251,6 +253,19 @@ def energy_surface(tr_xyz, tr_q, tr_area, chrpos, atmchr, kappa, eps, eps0, x, n
                             cp.shape[0], cp.ravel(), _d(atmchr).ravel(), kappa, eps, eps0,
                             _d(x).ravel(), C.byref(se), C.byref(ce), int(nthreads))
     return se.value, ce.value
+
+
+def output_potential(sptpos, nvert, tr_xyz, x_orig):
+    """main.f90:226-326: vertex potentials (nspt, 2) and the scaled face
+    values (2 nface), from x and the centroids in the ORIGINAL face order."""
+    sp = _d(sptpos).reshape(-1, 3)
+    nv = _i(nvert).reshape(-1, 3)
+    xyz = _d(tr_xyz).reshape(-1, 3)
+    vert = np.zeros((sp.shape[0], 2))
+    xs = np.zeros(2 * nv.shape[0])
+    lib().or_output_potential(sp.shape[0], sp.ravel(), nv.shape[0], nv.ravel(), xyz.ravel(),
+                              _d(x_orig).ravel(), vert.ravel(), xs)
+    return vert, xs
 
 
 def dgetrf(a):

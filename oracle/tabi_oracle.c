@@ -1535,3 +1535,43 @@ void or_energy(const or_tree* t, int nchr, const double* chrpos,
                     eps0, x, soleng, couleng, nthreads);
   free(xyz);
 }
+
+/* main.f90:226-326 output_potential: x_orig (2 nface, original face order)
+ * and the face centroids tr_xyz (3 x nface, original order) in; per vertex
+ * the first 14 faces using it in face order (the 15-row ind_vert table,
+ * :243,255-266), weighted by the inverse centroid distance (:268-281), then
+ * both vertex and face values times para*4*pi (:297-298). */
+void or_output_potential(int nspt, const double* sptpos, int nface, const int* nvert,
+                         const double* tr_xyz, const double* x_orig, double* vert_ptl,
+                         double* x_scaled) {
+  const int nface_vert = 15;
+  int* ind = (int*)calloc((size_t)nface_vert * (size_t)nspt, sizeof(int));
+  for (int i = 0; i < nface; ++i)
+    for (int j = 0; j < 3; ++j) {
+      int v = nvert[3 * i + j] - 1;
+      for (int k = 0; k < nface_vert - 1; ++k)
+        if (ind[(size_t)v * nface_vert + k] == 0) {
+          ind[(size_t)v * nface_vert + k] = i + 1;
+          ind[(size_t)v * nface_vert + nface_vert - 1] += 1;
+          break;
+        }
+    }
+  const double pi = acos(-1.0);
+  const double para_temp = 332.0716 * 4 * pi;
+  for (int i = 0; i < nspt; ++i) {
+    double tot = 0.0, v1 = 0.0, v2 = 0.0;
+    for (int j = 0; j < ind[(size_t)i * nface_vert + nface_vert - 1]; ++j) {
+      int f = ind[(size_t)i * nface_vert + j] - 1;
+      double aa[3];
+      for (int d = 0; d < 3; ++d) aa[d] = tr_xyz[3 * (size_t)f + d] - sptpos[3 * (size_t)i + d];
+      double ll = sqrt(dot3(aa, aa));
+      v1 = v1 + 1.0 / ll * x_orig[f];
+      v2 = v2 + 1.0 / ll * x_orig[f + nface];
+      tot = tot + 1.0 / ll;
+    }
+    vert_ptl[2 * (size_t)i] = v1 / tot * para_temp;
+    vert_ptl[2 * (size_t)i + 1] = v2 / tot * para_temp;
+  }
+  for (int i = 0; i < 2 * nface; ++i) x_scaled[i] = x_orig[i] * para_temp;
+  free(ind);
+}

@@ -123,6 +123,11 @@ void or_energy_surface(int nface, const double* tr_xyz, const double* tr_q,
 /* main.f90:62-65 constants: kappa from the REAL*4 literal 8.430325455. */
 double or_kappa(double bulk_strength, double eps1);
 
+/* main.f90:226-326 output_potential (vertex potentials; see tabi_oracle.c) */
+void or_output_potential(int nspt, const double* sptpos, int nface, const int* nvert,
+                         const double* tr_xyz, const double* x_orig, double* vert_ptl,
+                         double* x_scaled);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,7 @@ CSRC = os.path.join(PKG, "csrc")
 OUT = os.path.join(PKG, "_build")
 LIB = os.path.join(OUT, "libtabi_gpu.so")
 SOURCES = ["tree.cu", "matvec.cu", "precond.cu", "gmres.cu", "rhs_energy.cu", "tabi_api.cu",
-           "warmstart.cu", "noalloc.cu"]
+           "warmstart.cu", "potential.cu", "noalloc.cu"]
 HEADERS = ["tabi_impl.cuh", "taylor_gen.cuh", "bie_kernels.cuh", "reduce.cuh", "warmstart.cuh"]
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 

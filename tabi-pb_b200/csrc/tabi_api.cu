@@ -734,6 +734,43 @@ int tabi_probe_fp64_peak(double ms, double* flops) {
   });
 }
 
+// ---- output_potential (main.f90:226-326)
+int tabi_output_potential_dev(tabi_h h, int nspt, const double* sptpos_dev, int nface,
+                              const int* nvert_dev, const double* x_dev, double* x_orig_dev,
+                              double* vert_ptl_dev, void* stream) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    set_device(H);
+    output_potential_dev(H, nspt, sptpos_dev, nface, nvert_dev, x_dev, x_orig_dev, vert_ptl_dev,
+                         pick(H, stream));
+  });
+}
+
+int tabi_output_potential(tabi_h h, int nspt, const double* sptpos, int nface, const int* nvert,
+                          const double* x, double* x_orig, double* vert_ptl) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(sptpos && nvert && x && x_orig && vert_ptl && nspt > 0 && nface > 0,
+                 TABI_ERR_ARG, "null argument");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    h2d(H.vp_pos, sptpos, 3 * (size_t)nspt, s);
+    h2d(H.vp_nv, nvert, 3 * (size_t)nface, s);
+    h2d(H.vp_xo, x, 2 * (size_t)nface, s);  // x in tree order
+    H.vp_vert.alloc(2 * (size_t)nspt);
+    H.d_tmp.alloc(2 * (size_t)nface);
+    output_potential_dev(H, nspt, H.vp_pos.p, nface, H.vp_nv.p, H.vp_xo.p, H.d_tmp.p,
+                         H.vp_vert.p, s);
+    TABI_CUDA(cudaMemcpyAsync(x_orig, H.d_tmp.p, sizeof(double) * 2 * nface,
+                              cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaMemcpyAsync(vert_ptl, H.vp_vert.p, sizeof(double) * 2 * nspt,
+                              cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
 // ---- learned warm start
 // NULL = the CUDA default stream, as for any CUDA call
 static cudaStream_t ws_stream(tabi_ws, void* stream) { return (cudaStream_t)stream; }

@@ -286,6 +286,9 @@ struct Handle {
   DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;
   DBuf<int> st_fv;
   DBuf<double> rn_b0, rn_b, rn_x, rn_z;
+  // output_potential
+  DBuf<double> vp_cen, vp_xo, vp_vert, vp_pos;
+  DBuf<int> vp_cnt, vp_off, vp_list, vp_err, vp_scan, vp_nv;
 };
 
 // ---- kernels / launchers (defined in the .cu files) ----
@@ -305,6 +308,10 @@ double asum_dev(Handle& H, const double* x, int n, cudaStream_t s);
 // preconditioner (precond.cu)
 void build_precond(Handle& H, cudaStream_t s);
 void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s);
+// output_potential (potential.cu): x in tree order -> x_orig (2 n, original
+// face order) and vert_ptl (2 per vertex), both scaled by 332.0716 * 4 pi
+void output_potential_dev(Handle& H, int nspt, const double* sptpos, int nface, const int* nvert,
+                          const double* x, double* x_orig, double* vert_ptl, cudaStream_t s);
 // gmres (gmres.cu)
 void gmres_dev(Handle& H, const double* b, double* x, int* iter, double* err, int* ierr,
                double* hist, int* nhist, cudaStream_t s, double tol = -1.0);

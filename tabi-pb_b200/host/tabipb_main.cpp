@@ -281,54 +281,21 @@ int main(int argc, char** argv) {
   std::printf(" Solvation energy=: %24.16e  kcal/mol\n", soleng);
   std::printf(" -----Free energy=: %24.16e  kcal/mol \n", couleng + soleng);
 
-  // ---- output_potential (main.f90:226-326)
+  // ---- output_potential (main.f90:226-326): on the GPU (tabi_output_potential),
+  // the summary prints and the file writer here
   {
-    std::vector<double> xo(ndim), xyz_o(3 * (size_t)nface);
-    for (int i = 0; i < nface; ++i) {
-      int o = orderarr[i] - 1;
-      xo[o] = xvct[i];
-      xo[o + nface] = xvct[i + nface];
-      for (int d = 0; d < 3; ++d) xyz_o[3 * o + d] = tr_xyz[3 * i + d];
-    }
-    const int nface_vert = 15;
-    std::vector<int> ind_vert((size_t)nface_vert * nspt, 0);
-    auto IV = [&](int k, int v) -> int& { return ind_vert[(size_t)v * nface_vert + k]; };
-    for (int i = 0; i < nface; ++i)
-      for (int j = 0; j < 3; ++j) {
-        int v = nvert[3 * i + j] - 1;
-        for (int k = 0; k < nface_vert - 1; ++k)
-          if (IV(k, v) == 0) {
-            IV(k, v) = i + 1;
-            IV(nface_vert - 1, v) += 1;
-            break;
-          }
-      }
-    std::vector<double> vert_ptl(2 * (size_t)nspt, 0.0);
-    for (int i = 0; i < nspt; ++i) {
-      double tot = 0.0;
-      for (int j = 0; j < IV(nface_vert - 1, i); ++j) {
-        int f = IV(j, i) - 1;
-        double ll = dist3(&xyz_o[3 * (size_t)f], &sptpos[3 * (size_t)i]);
-        vert_ptl[2 * i] += 1.0 / ll * xo[f];
-        vert_ptl[2 * i + 1] += 1.0 / ll * xo[f + nface];
-        tot += 1.0 / ll;
-      }
-      vert_ptl[2 * i] /= tot;
-      vert_ptl[2 * i + 1] /= tot;
-    }
-    const double pt = para * 4 * pi;
+    std::vector<double> xo(ndim), vert_ptl(2 * (size_t)nspt);
+    check(h, tabi_output_potential(h, nspt, sptpos.data(), nface, nvert.data(), xvct.data(),
+                                xo.data(), vert_ptl.data()),
+          "tabi_output_potential");
     double emax[4] = {-1e300, -1e300, -1e300, -1e300}, emin[4] = {1e300, 1e300, 1e300, 1e300};
     for (int i = 0; i < nface; ++i) {
-      xo[i] *= pt;
-      xo[i + nface] *= pt;
       emax[0] = std::max(emax[0], xo[i]);
       emin[0] = std::min(emin[0], xo[i]);
       emax[1] = std::max(emax[1], xo[i + nface]);
       emin[1] = std::min(emin[1], xo[i + nface]);
     }
     for (int i = 0; i < nspt; ++i) {
-      vert_ptl[2 * i] *= pt;
-      vert_ptl[2 * i + 1] *= pt;
       emax[2] = std::max(emax[2], vert_ptl[2 * i]);
       emin[2] = std::min(emin[2], vert_ptl[2 * i]);
       emax[3] = std::max(emax[3], vert_ptl[2 * i + 1]);

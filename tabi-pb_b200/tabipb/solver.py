@@ -10,6 +10,7 @@ method by method (same names, same argument meaning, same array layouts):
     msolve(r)                  MSOLVEdric / MSOLVEprec, main.f90:511-542
     dgmres(b)                  DGMRES call, main.f90:92-139
     energy(x)                  main.f90:144-159 (+ potential_molecule)
+    output_potential(x)        main.f90:226-326
 
 All numerics run on the GPU; errors from the library raise TabiError.
 """
@@ -172,6 +173,20 @@ class TabiSolver:
         check(self.h, self.L.tabi_energy(self.h, cp.shape[0], dptr(cp), dptr(q), dptr(x),
                                          C.byref(se), C.byref(ce)))
         return se.value, ce.value
+
+    # ---- main.f90:226-326
+    def output_potential(self, sptpos, nvert, x):
+        """x (tree order, as dgmres returns it) -> (x in the original face order
+        and vertex values (nspt, 2): potential, normal derivative), both scaled
+        by 332.0716 * 4 pi as the reference writes them."""
+        sp = f64(sptpos, (-1, 3))
+        nv = i32(nvert).reshape(-1, 3)
+        x = f64(x).ravel()
+        xo = np.zeros_like(x)
+        vert = np.zeros((sp.shape[0], 2))
+        check(self.h, self.L.tabi_output_potential(self.h, sp.shape[0], dptr(sp), nv.shape[0],
+                                                   iptr(nv), dptr(x), dptr(xo), dptr(vert)))
+        return xo, vert
 
     def counts(self):
         a, b = C.c_int64(), C.c_int64()

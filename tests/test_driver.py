@@ -47,3 +47,10 @@ def test_driver_matches_library(gpu_lib, tmp_path):
                                 kappa=tabipb.kappa(0.15, 80.0), eps0=1.0, eps1=80.0)
     assert res["ierr"] == 0
     assert abs(se - res["soleng"]) <= 1e-9 * abs(res["soleng"]), (se, res["soleng"])
+    # vertex potentials of surface_potential.dat (main.f90:307-312), against
+    # the oracle's output_potential of the same solution
+    xyz_o, _, _, _ = O.form_matrix(pos, nrm, fc, xyz32, q32, 1.0)
+    vert_ref, _ = O.output_potential(pos, fc, xyz_o, res["x_orig"])
+    vert_dat = np.array([[float(t) for t in line.split()[7:9]] for line in dat[1:1 + nspt]])
+    ok = np.isfinite(vert_ref[:, 0])
+    np.testing.assert_allclose(vert_dat[ok], vert_ref[ok], rtol=1e-7, atol=2e-10)

@@ -161,3 +161,22 @@ def test_solve_and_energy(setup):
                         nthreads=8)
     assert abs(se - ose) <= ENERGY_TOL * abs(ose)
     assert abs(ce - oce) <= 1e-12 * max(abs(oce), 1e-30)
+
+
+def test_output_potential(setup):
+    """main.f90:226-326: vertex potentials and the scaled face values, GPU vs
+    oracle (same solution vector, un-permuted by orderarr)."""
+    import oracle as O
+
+    name, case, s, T, kap, g, o = setup
+    xyz, tq, ar, b = g
+    n = len(ar)
+    rng = np.random.default_rng(4)
+    x_tree = rng.standard_normal(2 * n)
+    xo_gpu, vert_gpu = s.output_potential(case["sptpos"], case["nvert"], x_tree)
+    x_orig = _from_tree(x_tree, s.orderarr, n)
+    vert_ref, xs_ref = O.output_potential(case["sptpos"], case["nvert"], xyz, x_orig)
+    np.testing.assert_array_equal(xo_gpu, xs_ref)
+    used = np.isfinite(vert_ref[:, 0])
+    np.testing.assert_array_equal(np.isfinite(vert_gpu[:, 0]), used)
+    np.testing.assert_allclose(vert_gpu[used], vert_ref[used], rtol=1e-14, atol=0)
