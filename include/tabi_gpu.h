@@ -210,6 +210,17 @@ const char* tabi_profile_class_name(int kclass);
  * returns the achieved FP64 FLOP/s (2 per FMA). */
 int tabi_probe_fp64_peak(double ms, double* flops);
 
+/* One shard of the operator (no counterpart in the reference, which is serial):
+ * after tabi_build_tree, restricts tabi_matvec(_dev) and tabi_msolve(_dev) to
+ * the targets [t0, t1) of the tree order (0-based, half-open, starting and
+ * ending on leaf boundaries): only those entries of y / z are written, the
+ * far and near interactions and the leaf blocks of other targets are not
+ * computed (the cluster moments still are: every shard needs all of them).
+ * The shards' slices then assemble the full vector (an all-gather), and the
+ * solve runs across shards; tabi_solve on a restricted handle is refused.
+ * (0, nface) lifts the restriction. */
+int tabi_set_target_range(tabi_h h, int t0, int t1);
+
 /* main.f90:226-326 output_potential, after tabi_build_tree: x (2 nface) is
  * the solution in tree order as tabi_solve returns it; x_orig receives it in
  * the original face order and vert_ptl (2 per vertex: potential, normal

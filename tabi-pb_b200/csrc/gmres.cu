@@ -404,6 +404,9 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
 // which also bounds the inner iterations in total).
 void solve_dev(Handle& H, const double* b, double* x, int* iter_out, double* err_out,
                int* ierr_out, double* hist, int* nhist, cudaStream_t s) {
+  TABI_REQUIRE(!H.tree.ranged, TABI_ERR_STATE,
+               "a target range is set: the handle computes one shard of the operator, the "
+               "solve runs across the shards (tabipb.sharded)");
   if (H.prm.precision != TABI_PREC_MIXED) {
     H.mv_prec = TABI_PREC_FP64;
     gmres_dev(H, b, x, iter_out, err_out, ierr_out, hist, nhist, s);

@@ -19,6 +19,8 @@
 //               y1 = pre1*x1 - peng1, y2 = pre2*x2 - peng2 (:1177-1178).
 // All results are written to per-(target, interaction) slots fixed by the
 // traversal, so the sums are deterministic.
+#include <algorithm>
+
 #include "bie_kernels.cuh"
 #include "reduce.cuh"
 #include "taylor_gen.cuh"
@@ -324,9 +326,10 @@ __global__ void __launch_bounds__(kNearThreads) near_kernel_f32(
 
 __global__ void reduce_kernel(const int64_t* __restrict__ slot_off,
                               const double2* __restrict__ res, const double* __restrict__ x,
-                              int n, double pre1, double pre2, double* __restrict__ y) {
-  int t = blockIdx.x * blockDim.x + threadIdx.x;
-  if (t >= n) return;
+                              int n, int t0, int t1, double pre1, double pre2,
+                              double* __restrict__ y) {
+  int t = t0 + blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= t1) return;
   double s1 = 0.0, s2 = 0.0;
   for (int64_t k = slot_off[t]; k < slot_off[t + 1]; ++k) {
     double2 r = res[k];
@@ -363,16 +366,19 @@ void launch_moments(Handle& H, const double* x, bool f32, cudaStream_t s) {
 template <int P>
 void launch_far(Handle& H, bool f32, cudaStream_t s) {
   Tree& T = H.tree;
-  if (T.far_work.empty()) return;
+  const int nw = (int)(T.ranged ? T.r_far_work.size() : T.far_work.size());
+  const WorkItem* fw = T.ranged ? T.d_r_far_work.p : T.d_far_work.p;
+  const int2* fe = T.ranged ? T.d_r_far_ent.p : T.d_far_ent.p;
+  if (nw == 0) return;
   const double eps = H.prm.eps1 / H.prm.eps0;
   TABI_K(K_FAR, s);
   if (f32)
-    far_kernel<P, float><<<(int)T.far_work.size(), 64, 0, s>>>(
-        T.d_far_work.p, T.d_far_ent.p, H.d_mwf.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p,
+    far_kernel<P, float><<<nw, 64, 0, s>>>(
+        fw, fe, H.d_mwf.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p,
         H.d_nx.p, H.d_ny.p, H.d_nz.p, (float)H.prm.kappa, (float)eps, H.d_res.p);
   else
-    far_kernel<P, double><<<(int)T.far_work.size(), 64, 0, s>>>(
-        T.d_far_work.p, T.d_far_ent.p, H.d_mw.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p,
+    far_kernel<P, double><<<nw, 64, 0, s>>>(
+        fw, fe, H.d_mw.p, T.d_mid.p, H.d_x.p, H.d_y.p, H.d_z.p,
         H.d_nx.p, H.d_ny.p, H.d_nz.p, H.prm.kappa, eps, H.d_res.p);
 }
 
@@ -446,7 +452,10 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
   TABI_PHASE(K_PHASE_MATVEC, s);
   // the near field runs on the handle's side stream, concurrently with the
   // moments + far field on s; both write disjoint result slots
-  const bool fork = !T.near_work.empty() && H.side != nullptr;
+  const int nnw = (int)(T.ranged ? T.r_near_work.size() : T.near_work.size());
+  const WorkItem* nwk = T.ranged ? T.d_r_near_work.p : T.d_near_work.p;
+  const int2* nent = T.ranged ? T.d_r_near_ent.p : T.d_near_ent.p;
+  const bool fork = nnw > 0 && H.side != nullptr;
   cudaStream_t sn = fork ? H.side : s;
   if (fork) {
     TABI_CUDA(cudaEventRecord(H.ev_fork, s));
@@ -465,16 +474,16 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
     case 8: launch_moments<8>(H, x, f32, s); break;
     default: throw Error(TABI_ERR_ARG, "order must be 1..8");
   }
-  if (!T.near_work.empty() && f32) {
+  if (nnw > 0 && f32) {
     TABI_K(K_NEAR, sn);
-    near_kernel_f32<<<(int)T.near_work.size(), kNearThreads, 0, sn>>>(
-        T.d_near_work.p, T.d_near_ent.p, T.d_ibeg.p, T.d_num.p, T.d_mid.p, H.d_x.p, H.d_y.p,
+    near_kernel_f32<<<nnw, kNearThreads, 0, sn>>>(
+        nwk, nent, T.d_ibeg.p, T.d_num.p, T.d_mid.p, H.d_x.p, H.d_y.p,
         H.d_z.p, T.d_lpos.p, T.d_llo.p, T.d_lnrm.p, x, n, (float)H.prm.kappa,
         (float)(H.prm.eps1 / H.prm.eps0), H.d_res.p);
-  } else if (!T.near_work.empty()) {
+  } else if (nnw > 0) {
     TABI_K(K_NEAR, sn);
-    near_kernel<<<(int)T.near_work.size(), kNearThreads, 0, sn>>>(
-        T.d_near_work.p, T.d_near_ent.p, T.d_ibeg.p, T.d_num.p, H.d_x.p, H.d_y.p, H.d_z.p,
+    near_kernel<<<nnw, kNearThreads, 0, sn>>>(
+        nwk, nent, T.d_ibeg.p, T.d_num.p, H.d_x.p, H.d_y.p, H.d_z.p,
         H.d_nx.p, H.d_ny.p, H.d_nz.p, H.d_area.p, x, n, H.prm.kappa, H.prm.eps1 / H.prm.eps0,
         H.d_res.p);
   }
@@ -494,9 +503,81 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
     TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
   }
   double eps = H.prm.eps1 / H.prm.eps0;
-  { TABI_K(K_REDUCE, s); reduce_kernel<<<ceil_div(n, 256), 256, 0, s>>>(T.d_slot_off.p, H.d_res.p, x, n,
+  const int t0 = T.ranged ? T.rt0 : 0, t1 = T.ranged ? T.rt1 : n;
+  { TABI_K(K_REDUCE, s); reduce_kernel<<<ceil_div(t1 - t0, 256), 256, 0, s>>>(T.d_slot_off.p, H.d_res.p, x, n, t0, t1,
                                                  0.5 * (1.0 + eps), 0.5 * (1.0 + 1.0 / eps), y); }
   TABI_CUDA(cudaGetLastError());
+}
+
+void set_target_range(Handle& H, int t0, int t1, cudaStream_t s) {
+  Tree& T = H.tree;
+  const int n = H.n;
+  TABI_REQUIRE(H.has_tree, TABI_ERR_STATE, "tabi_build_tree has not been called");
+  TABI_REQUIRE(0 <= t0 && t0 < t1 && t1 <= n, TABI_ERR_ARG, "target range must be within 0..nface");
+  T.ranged = false;
+  if (t0 == 0 && t1 == n) return;
+  // leaf-aligned: the shard owns whole leaves (so the preconditioner, which is
+  // leaf-local, splits with it)
+  std::vector<int> starts;
+  for (int c : T.leaves) starts.push_back(T.ibeg[c]);
+  std::sort(starts.begin(), starts.end());
+  auto boundary = [&](int t) {
+    return t == n || std::binary_search(starts.begin(), starts.end(), t);
+  };
+  TABI_REQUIRE(boundary(t0) && boundary(t1), TABI_ERR_ARG,
+               "target range must start and end on leaf boundaries (tree order)");
+  // the interaction entries of targets in range, item by item
+  auto restrict_list = [&](const std::vector<WorkItem>& work, const DBuf<int2>& ent,
+                           std::vector<WorkItem>& rwork, DBuf<WorkItem>& d_rwork,
+                           DBuf<int2>& d_rent) {
+    size_t total = 0;
+    for (const WorkItem& w : work) total = std::max(total, (size_t)w.start + w.count);
+    std::vector<int2> h(total), out;
+    if (total)
+      TABI_CUDA(cudaMemcpyAsync(h.data(), ent.p, sizeof(int2) * total, cudaMemcpyDeviceToHost,
+                                s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+    rwork.clear();
+    for (const WorkItem& w : work) {
+      const int start = (int)out.size();
+      for (int k = 0; k < w.count; ++k) {
+        const int2 e = h[(size_t)w.start + k];
+        if (e.x >= t0 && e.x < t1) out.push_back(e);
+      }
+      const int cnt = (int)out.size() - start;
+      if (cnt > 0) rwork.push_back(WorkItem{w.node, start, cnt, w.mslot});
+    }
+    d_rwork.alloc(std::max<size_t>(rwork.size(), 1));
+    d_rent.alloc(std::max<size_t>(out.size(), 1));
+    if (!rwork.empty())
+      TABI_CUDA(cudaMemcpyAsync(d_rwork.p, rwork.data(), sizeof(WorkItem) * rwork.size(),
+                                cudaMemcpyHostToDevice, s));
+    if (!out.empty())
+      TABI_CUDA(cudaMemcpyAsync(d_rent.p, out.data(), sizeof(int2) * out.size(),
+                                cudaMemcpyHostToDevice, s));
+  };
+  restrict_list(T.far_work, T.d_far_ent, T.r_far_work, T.d_r_far_work, T.d_r_far_ent);
+  restrict_list(T.near_work, T.d_near_ent, T.r_near_work, T.d_r_near_work, T.d_r_near_ent);
+  // the preconditioner's leaves in range, in the apply's big / small classes
+  std::vector<int> big, small;
+  for (int l = 0; l < T.nleaf; ++l) {
+    const int c = T.leaves[l], b0 = T.ibeg[c], nm = T.num[c];
+    if (b0 >= t0 && b0 + nm <= t1) (2 * nm > 512 ? big : small).push_back(l);
+  }
+  auto by_size = [&](int a, int b) { return T.num[T.leaves[a]] > T.num[T.leaves[b]]; };
+  std::sort(big.begin(), big.end(), by_size);
+  std::sort(small.begin(), small.end(), by_size);
+  T.r_solve_big = (int)big.size();
+  T.r_solve_small = (int)small.size();
+  big.insert(big.end(), small.begin(), small.end());
+  T.d_r_solve_list.alloc(std::max<size_t>(big.size(), 1));
+  if (!big.empty())
+    TABI_CUDA(cudaMemcpyAsync(T.d_r_solve_list.p, big.data(), sizeof(int) * big.size(),
+                              cudaMemcpyHostToDevice, s));
+  TABI_CUDA(cudaStreamSynchronize(s));
+  T.ranged = true;
+  T.rt0 = t0;
+  T.rt1 = t1;
 }
 
 }  // namespace tabi

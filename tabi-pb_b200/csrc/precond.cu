@@ -1156,23 +1156,27 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
     raise_smem_limit((const void*)solve_kernel<256>, smem);
     raise_smem_limit((const void*)solve_kernel<512>, smem);
   }
-  const bool fork = T.n_solve_big > 0 && T.n_solve_small > 0 && H.side != nullptr;
+  // a shard applies the leaves of its target range only
+  const int nbig = T.ranged ? T.r_solve_big : T.n_solve_big;
+  const int nsmall = T.ranged ? T.r_solve_small : T.n_solve_small;
+  const int* list = T.ranged ? T.d_r_solve_list.p : T.d_solve_list.p;
+  const bool fork = nbig > 0 && nsmall > 0 && H.side != nullptr;
   cudaStream_t s2 = fork ? H.side : s;
   if (fork) {
     TABI_CUDA(cudaEventRecord(H.ev_fork, s));
     TABI_CUDA(cudaStreamWaitEvent(s2, H.ev_fork, 0));
   }
-  if (T.n_solve_big > 0) {
+  if (nbig > 0) {
     TABI_K(K_SOLVE, s);
-    solve_kernel<512><<<T.n_solve_big, 512, smem, s>>>(
-        T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_solve_list.p, T.d_lu.p, T.d_dinv.p,
-        T.d_lu_perm.p, n, r, z);
+    solve_kernel<512><<<nbig, 512, smem, s>>>(T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p,
+                                              list, T.d_lu.p, T.d_dinv.p, T.d_lu_perm.p, n, r,
+                                              z);
   }
-  if (T.n_solve_small > 0) {
+  if (nsmall > 0) {
     TABI_K(K_SOLVE, s2);
-    solve_kernel<256><<<T.n_solve_small, 256, smem, s2>>>(
-        T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_solve_list.p + T.n_solve_big,
-        T.d_lu.p, T.d_dinv.p, T.d_lu_perm.p, n, r, z);
+    solve_kernel<256><<<nsmall, 256, smem, s2>>>(T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p,
+                                                 list + nbig, T.d_lu.p, T.d_dinv.p,
+                                                 T.d_lu_perm.p, n, r, z);
   }
   if (fork) {
     TABI_CUDA(cudaEventRecord(H.ev_join, s2));

@@ -734,6 +734,16 @@ int tabi_probe_fp64_peak(double ms, double* flops) {
   });
 }
 
+// ---- shards of the operator
+int tabi_set_target_range(tabi_h h, int t0, int t1) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    set_device(H);
+    set_target_range(H, t0, t1, H.stream);
+  });
+}
+
 // ---- output_potential (main.f90:226-326)
 int tabi_output_potential_dev(tabi_h h, int nspt, const double* sptpos_dev, int nface,
                               const int* nvert_dev, const double* x_dev, double* x_orig_dev,

@@ -102,6 +102,9 @@ struct Tree {
     n_solve_big = n_solve_small = 0;
     max_leaf = 0;
     lrel_ready = false;
+    ranged = false;
+    r_far_work.clear();
+    r_near_work.clear();
   }
   int n = 0;          // faces
   int nnodes = 0;
@@ -147,6 +150,15 @@ struct Tree {
   DBuf<int> d_leaves;
   DBuf<float4> d_lpos, d_llo, d_lnrm;
   bool lrel_ready = false;
+  // a shard's target range (tabi_set_target_range): the interaction lists
+  // restricted to targets [rt0, rt1) and the leaves inside it
+  bool ranged = false;
+  int rt0 = 0, rt1 = 0;
+  std::vector<WorkItem> r_far_work, r_near_work;
+  DBuf<WorkItem> d_r_far_work, d_r_near_work;
+  DBuf<int2> d_r_far_ent, d_r_near_ent;
+  DBuf<int> d_r_solve_list;
+  int r_solve_big = 0, r_solve_small = 0;
 };
 
 // Kernel classes for the launch counters / event timers (tabi_profile_*).
@@ -304,6 +316,9 @@ void build_tree(Handle& H, cudaStream_t s);
 void build_lists(Handle& H, cudaStream_t s);
 // matvec (matvec.cu)
 void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool check_zero);
+// restricts matvec_dev / msolve_dev to the leaf-aligned target range [t0, t1)
+// of the tree order (the whole range lifts the restriction)
+void set_target_range(Handle& H, int t0, int t1, cudaStream_t s);
 double asum_dev(Handle& H, const double* x, int n, cudaStream_t s);
 // preconditioner (precond.cu)
 void build_precond(Handle& H, cudaStream_t s);

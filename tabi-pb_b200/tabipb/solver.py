@@ -174,6 +174,20 @@ class TabiSolver:
                                          C.byref(se), C.byref(ce)))
         return se.value, ce.value
 
+    # ---- shards of the operator
+    def leaves(self):
+        """(start, size) of each leaf in tree order (0-based starts)."""
+        t = self.tree_nodes()
+        m = t["nchild"] == 0
+        st = t["ibeg"][m] - 1
+        o = np.argsort(st, kind="stable")
+        return st[o].astype(np.int64), t["numpar"][m][o].astype(np.int64)
+
+    def set_target_range(self, t0, t1):
+        """Restrict matvec / msolve to the tree-order targets [t0, t1)
+        (leaf-aligned): only that slice of y / z is written."""
+        check(self.h, self.L.tabi_set_target_range(self.h, int(t0), int(t1)))
+
     # ---- main.f90:226-326
     def output_potential(self, sptpos, nvert, x):
         """x (tree order, as dgmres returns it) -> (x in the original face order
