@@ -355,6 +355,7 @@ def gpu_arm(args):
     e2e_solver.close()
 
     batched = batched_leg(args, dev, rank) if args.batch > 0 else None
+    large = large_leg(args, dev) if (args.large and rank == 0) else None
 
     out = None
     if rank == 0:
@@ -411,6 +412,8 @@ def gpu_arm(args):
             out["mixed_learned"] = learned
         if batched is not None:
             out["batched"] = batched
+        if large is not None:
+            out["large_mixed"] = large
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
@@ -422,6 +425,79 @@ def gpu_arm(args):
     if out is not None:
         print(json.dumps(out), flush=True)
     solver.close()
+
+
+# ---------------------------------------------------------------- large mixed leg
+LARGE = dict(natm=20000, radius=40.0, min_sep=2.0, density=10.0, probe=1.4, seed=0, order=6,
+             theta=0.7, maxparnode=400, tol=1e-6, eps0=1.0, eps1=80.0, bulk=0.15,
+             name="large-20000-atoms-40A-10vA2-p6-mac0.7-leaf400-mixed-tol1e-6")
+
+
+def large_leg(args, dev):
+    """The large mixed-precision configuration: 20,000 atoms in 40 A (same
+    generator, 10 vertices/A^2), order 6, MAC 0.7, leaf 400, FP32 treecode with
+    FP64 refinement to 1e-6 (FP64 residual measure).  Reported: solves/s (one
+    timed solve after one warm-up), iterations, and the operator's error
+    against the FP64 direct sum (tabi_direct_targets) at 10,000 sampled
+    targets, for the FP32 and the FP64 treecode."""
+    import torch
+
+    import tabipb
+    from tabipb import surface as S
+
+    w = LARGE
+    xyz, q, r = S.synthetic_molecule(w["natm"], w["radius"], min_sep=w["min_sep"], seed=w["seed"])
+    pos, nrm, fc, _ = S.gaussian_surface(xyz, r, density=w["density"], probe=w["probe"])
+    fc, _ = S.face_filter(pos, fc)
+    nspt, nface, natm = len(pos), len(fc), len(q)
+    f = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
+    d = dict(sptpos=f(pos), sptnrm=f(nrm), nvert=f(np.asarray(fc, np.int32)), chrpos=f(xyz),
+             atmchr=f(q))
+    kap = tabipb.kappa(w["bulk"], w["eps1"])
+    prm = dict(order=w["order"], maxparnode=w["maxparnode"], theta=w["theta"], kappa=kap,
+               eps0=w["eps0"], eps1=w["eps1"], tol=w["tol"])
+    s32 = tabipb.TabiSolver(precision=tabipb.PREC_MIXED, **prm)
+    x = torch.zeros(2 * nface, dtype=torch.float64, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def run():
+        return s32.run_dev(nspt, d["sptpos"].data_ptr(), d["sptnrm"].data_ptr(), nface,
+                           d["nvert"].data_ptr(), natm, d["chrpos"].data_ptr(),
+                           d["atmchr"].data_ptr(), x.data_ptr(), stream.cuda_stream)
+
+    run()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    res = run()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    xt = x.cpu().numpy()
+    rng = np.random.default_rng(11)
+    tg = np.sort(rng.choice(nface, min(10000, nface), replace=False)).astype(np.int32)
+    yd1, yd2 = s32.direct_targets(tg, xt)
+    y32 = s32.matvec(xt)
+    s64 = tabipb.TabiSolver(**prm)
+    s64.form_matrix(pos, nrm, fc, xyz, q)
+    s64.build_tree()
+    y64 = s64.matvec(xt)
+    s64.close()
+    s32.close()
+    yd = np.concatenate([yd1, yd2])
+    pick = lambda y: np.concatenate([y[tg], y[nface + tg]])
+    rel = lambda y: float(np.linalg.norm(pick(y) - yd) / np.linalg.norm(yd))
+    return {"value": 1e3 / ms, "unit": "solves/s", "ms_per_solve": ms, "workload": w["name"],
+            "faces": nface, "atoms": natm, "gmres_iterations": res["iter"],
+            "fp64_residual_measure": res["err"], "ierr": res["ierr"],
+            "soleng_kcal_mol": res["soleng"], "near_pairs_per_matvec": res["near_pairs"],
+            "far_per_matvec": res["far"],
+            "operator_rel_error_vs_fp64_direct_sum": {"targets": int(tg.size),
+                                                      "fp32_treecode": rel(y32),
+                                                      "fp64_treecode": rel(y64)},
+            "note": "the generator at 10 vertices/A^2 gives this face count for 20,000 atoms "
+                    "in 40 A"}
 
 
 # ---------------------------------------------------------------- batched leg
@@ -545,6 +621,8 @@ def main():
     ap.add_argument("--batch", type=int, default=16,
                     help="molecules in the batched leg (0 skips it)")
     ap.add_argument("--batch-workers", type=int, default=4)
+    ap.add_argument("--no-large", dest="large", action="store_false",
+                    help="skip the large mixed-precision leg (20,000 atoms, order 6, tol 1e-6)")
     ap.add_argument("--iters", type=int, default=27,
                     help="GMRES iterations used to scale the reference-arm sample")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="globular")

@@ -210,6 +210,15 @@ const char* tabi_profile_class_name(int kclass);
  * returns the achieved FP64 FLOP/s (2 per FMA). */
 int tabi_probe_fp64_peak(double ms, double* flops);
 
+/* Accuracy reference (no counterpart in the reference, whose treecode is
+ * checked against a direct sum only in its papers): the operator evaluated
+ * by an FP64 direct sum over every source (COMPP_DIRECT_PB's kernels,
+ * treecode3d_pb.f:919-1008, self term excluded) at nt targets of the current
+ * face order (0-based; the tree order after tabi_build_tree).  x is 2 nface;
+ * y receives [y1 of the targets; y2 of the targets] (2 nt).  Cost nt x nface
+ * pair evaluations on the GPU. */
+int tabi_direct_targets(tabi_h h, int nt, const int* targets, const double* x, double* y);
+
 /* One shard of the operator (no counterpart in the reference, which is serial):
  * after tabi_build_tree, restricts tabi_matvec(_dev) and tabi_msolve(_dev) to
  * the targets [t0, t1) of the tree order (0-based, half-open, starting and

@@ -509,6 +509,104 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
   TABI_CUDA(cudaGetLastError());
 }
 
+namespace {
+
+// FP64 direct sum of the operator for selected targets (the accuracy
+// reference of the treecode): y_t = pre x_t - sum_{j != t} (K(t, j) A_j x_j),
+// every source evaluated exactly (COMPP_DIRECT_PB's kernels,
+// treecode3d_pb.f:919-1008).  Grid: x = chunks of kDirT targets (one per
+// thread), y = chunks of kDirS sources staged through shared memory;
+// partials per (target, source chunk) are summed in chunk order afterwards.
+constexpr int kDirT = 128, kDirS = 8192, kDirTile = 256;
+
+__global__ void __launch_bounds__(kDirT) direct_kernel(
+    int n, const int* __restrict__ targets, int nt, const double* __restrict__ px,
+    const double* __restrict__ py, const double* __restrict__ pz,
+    const double* __restrict__ nx, const double* __restrict__ ny,
+    const double* __restrict__ nz, const double* __restrict__ area,
+    const double* __restrict__ x, double kappa, double eps, double2* __restrict__ part) {
+  __shared__ double s_x[kDirTile], s_y[kDirTile], s_z[kDirTile];
+  __shared__ double s_nx[kDirTile], s_ny[kDirTile], s_nz[kDirTile];
+  __shared__ double s_w1[kDirTile], s_w2[kDirTile];
+  const int k = blockIdx.x * kDirT + threadIdx.x;
+  const bool own = k < nt;
+  const int t = own ? targets[k] : 0;
+  const double tx = px[t], ty = py[t], tz = pz[t], vx = nx[t], vy = ny[t], vz = nz[t];
+  const double inv_eps = 1.0 / eps;
+  const int j0 = blockIdx.y * kDirS, j1 = min(n, j0 + kDirS);
+  double p1 = 0.0, p2 = 0.0;
+  for (int b0 = j0; b0 < j1; b0 += kDirTile) {
+    const int cnt = min(kDirTile, j1 - b0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt; q += kDirT) {
+      const int j = b0 + q;
+      s_x[q] = px[j];
+      s_y[q] = py[j];
+      s_z[q] = pz[j];
+      s_nx[q] = nx[j];
+      s_ny[q] = ny[j];
+      s_nz[q] = nz[j];
+      s_w1[q] = area[j] * x[j];
+      s_w2[q] = area[j] * x[n + j];
+    }
+    __syncthreads();
+    if (own)
+      for (int q = 0; q < cnt; ++q) {
+        const bool skip = (b0 + q == t);
+        double dx = s_x[q] - tx, dy = s_y[q] - ty, dz = s_z[q] - tz;
+        if (skip) dx = 1.0;
+        double K1, K2, K3, K4;
+        bie4<double>(dx, dy, dz, vx, vy, vz, s_nx[q], s_ny[q], s_nz[q], kappa, eps, inv_eps, K1,
+                     K2, K3, K4);
+        const double w1 = skip ? 0.0 : s_w1[q], w2 = skip ? 0.0 : s_w2[q];
+        p1 = fma(K1, w1, fma(K2, w2, p1));
+        p2 = fma(K3, w1, fma(K4, w2, p2));
+      }
+  }
+  if (own) part[(size_t)k * gridDim.y + blockIdx.y] = make_double2(p1, p2);
+}
+
+__global__ void direct_final_kernel(int n, const int* __restrict__ targets, int nt, int nchunk,
+                                    const double2* __restrict__ part,
+                                    const double* __restrict__ x, double pre1, double pre2,
+                                    double* __restrict__ y) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nt) return;
+  const int t = targets[k];
+  double s1 = 0.0, s2 = 0.0;
+  for (int c = 0; c < nchunk; ++c) {
+    const double2 r = part[(size_t)k * nchunk + c];
+    s1 += r.x;
+    s2 += r.y;
+  }
+  y[k] = pre1 * x[t] - s1;
+  y[nt + k] = pre2 * x[n + t] - s2;
+}
+
+}  // namespace
+
+void direct_targets_dev(Handle& H, int nt, const int* targets, const double* x, double* y,
+                        cudaStream_t s) {
+  TABI_REQUIRE(H.has_surface, TABI_ERR_STATE, "no surface");
+  const int n = H.n;
+  const int nchunk = ceil_div(n, kDirS);
+  H.d_dirpart.alloc((size_t)std::max(nt, 1) * nchunk);
+  const double eps = H.prm.eps1 / H.prm.eps0;
+  {
+    TABI_K(K_NEAR, s);
+    direct_kernel<<<dim3(ceil_div(nt, kDirT), nchunk), kDirT, 0, s>>>(
+        n, targets, nt, H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p, H.d_ny.p, H.d_nz.p, H.d_area.p, x,
+        H.prm.kappa, eps, H.d_dirpart.p);
+  }
+  {
+    TABI_K(K_REDUCE, s);
+    direct_final_kernel<<<ceil_div(nt, 256), 256, 0, s>>>(n, targets, nt, nchunk,
+                                                          H.d_dirpart.p, x, 0.5 * (1.0 + eps),
+                                                          0.5 * (1.0 + 1.0 / eps), y);
+  }
+  TABI_CUDA(cudaGetLastError());
+}
+
 void set_target_range(Handle& H, int t0, int t1, cudaStream_t s) {
   Tree& T = H.tree;
   const int n = H.n;

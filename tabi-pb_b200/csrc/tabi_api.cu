@@ -734,6 +734,27 @@ int tabi_probe_fp64_peak(double ms, double* flops) {
   });
 }
 
+// ---- accuracy reference
+int tabi_direct_targets(tabi_h h, int nt, const int* targets, const double* x, double* y) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(nt > 0 && targets && x && y, TABI_ERR_ARG, "null argument");
+    TABI_REQUIRE(H.has_surface, TABI_ERR_STATE, "no surface");
+    for (int k = 0; k < nt; ++k)
+      TABI_REQUIRE(targets[k] >= 0 && targets[k] < H.n, TABI_ERR_ARG, "target index out of range");
+    set_device(H);
+    cudaStream_t s = H.stream;
+    H.st_fv.alloc(nt);
+    TABI_CUDA(cudaMemcpyAsync(H.st_fv.p, targets, sizeof(int) * nt, cudaMemcpyHostToDevice, s));
+    h2d(H.st_x, x, 2 * (size_t)H.n, s);
+    H.d_tmp.alloc(2 * (size_t)nt);
+    direct_targets_dev(H, nt, H.st_fv.p, H.st_x.p, H.d_tmp.p, s);
+    TABI_CUDA(cudaMemcpyAsync(y, H.d_tmp.p, sizeof(double) * 2 * nt, cudaMemcpyDeviceToHost, s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+  });
+}
+
 // ---- shards of the operator
 int tabi_set_target_range(tabi_h h, int t0, int t1) {
   if (!h) return TABI_ERR_ARG;

@@ -265,6 +265,7 @@ struct Handle {
   DBuf<float> d_mwf;      // the same in FP32 (mixed-precision far field)
   int mv_prec = TABI_PREC_FP64;  // arithmetic of the treecode operator
   DBuf<double2> d_res;    // per-slot interaction results
+  DBuf<double2> d_dirpart;  // direct-sum partials (accuracy reference)
   DBuf<double> d_red;     // reduction scratch
   DBuf<double> h_red_pinned_dummy;
   double* h_pinned = nullptr;  // small pinned host scratch (64 doubles)
@@ -319,6 +320,10 @@ void matvec_dev(Handle& H, const double* x, double* y, cudaStream_t s, bool chec
 // restricts matvec_dev / msolve_dev to the leaf-aligned target range [t0, t1)
 // of the tree order (the whole range lifts the restriction)
 void set_target_range(Handle& H, int t0, int t1, cudaStream_t s);
+// FP64 direct sum of the operator at nt targets (current face order): y is
+// [y1 of the targets; y2 of the targets] (2 nt)
+void direct_targets_dev(Handle& H, int nt, const int* targets, const double* x, double* y,
+                        cudaStream_t s);
 double asum_dev(Handle& H, const double* x, int n, cudaStream_t s);
 // preconditioner (precond.cu)
 void build_precond(Handle& H, cudaStream_t s);

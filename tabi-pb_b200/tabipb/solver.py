@@ -174,6 +174,16 @@ class TabiSolver:
                                          C.byref(se), C.byref(ce)))
         return se.value, ce.value
 
+    # ---- accuracy reference
+    def direct_targets(self, targets, x):
+        """FP64 direct sum of the operator at the given targets (current face
+        order, 0-based): returns (y1, y2) of those targets."""
+        t = i32(targets).ravel()
+        x = f64(x).ravel()
+        y = np.zeros(2 * t.size)
+        check(self.h, self.L.tabi_direct_targets(self.h, t.size, iptr(t), dptr(x), dptr(y)))
+        return y[: t.size], y[t.size:]
+
     # ---- shards of the operator
     def leaves(self):
         """(start, size) of each leaf in tree order (0-based starts)."""

@@ -180,3 +180,22 @@ def test_output_potential(setup):
     used = np.isfinite(vert_ref[:, 0])
     np.testing.assert_array_equal(np.isfinite(vert_gpu[:, 0]), used)
     np.testing.assert_allclose(vert_gpu[used], vert_ref[used], rtol=1e-14, atol=0)
+
+
+def test_direct_sum_targets(setup):
+    """tabi_direct_targets (FP64 direct sum, the accuracy reference of the
+    treecode) against the oracle's direct sum, at sampled targets."""
+    import oracle as O
+
+    name, case, s, T, kap, g, o = setup
+    xyz, tq, ar, b = g
+    n = len(ar)
+    rng = np.random.default_rng(6)
+    x_tree = rng.standard_normal(2 * n)
+    tg = np.sort(rng.choice(n, min(n, 300), replace=False)).astype(np.int32)
+    y1, y2 = s.direct_targets(tg, x_tree)
+    # the oracle on the same (tree) face order
+    txyz, ttq, tar, _ = s.permute(xyz, tq, ar, b)
+    yd = O.matvec_direct(txyz, ttq, tar, kap, EPS1 / EPS0, x_tree)
+    np.testing.assert_allclose(y1, yd[tg], rtol=1e-12, atol=1e-12 * np.abs(yd).max())
+    np.testing.assert_allclose(y2, yd[n + tg], rtol=1e-12, atol=1e-12 * np.abs(yd).max())
