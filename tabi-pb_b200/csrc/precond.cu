@@ -261,7 +261,7 @@ constexpr int kPT = 256;           // panel kernel threads
 constexpr int kUT = 256;           // strip / gemm kernel threads
 constexpr int kUC = 128;           // strip width
 constexpr int kGT = 64;            // gemm tile
-constexpr int kOB = 128;           // outer block: columns right of it are updated once per block
+constexpr int kOB = 256;           // outer block: columns right of it are updated once per block
 constexpr int kPanelSmall = 320;   // rows left: panels up to this run in their own launch
 
 // Factor columns [c0l, c0l + nb) of the panel held in P (local column c of
@@ -657,7 +657,7 @@ __global__ void __launch_bounds__(256) lu_swapmap_kernel(const int* __restrict__
 
 // item = (slot, c0, c1, leaf): the outer block's row interchanges on columns
 // [c0, c1), through the map of lu_swapmap_kernel (slot = the leaf's map row)
-constexpr int kRC = 16;  // columns per pass
+constexpr int kRC = 8;  // columns per pass
 __global__ void __launch_bounds__(kUT) lu_rowswap_kernel(const int4* __restrict__ items,
                                                          const int2* __restrict__ leaf_rng,
                                                          const int64_t* __restrict__ blk_off,
