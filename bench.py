@@ -8,7 +8,7 @@ Workload (one "step" = one complete TABI-PB solve of one molecule):
   separation 2.0 A: 3 A is geometrically infeasible at that density), radii
   U(1.5, 2.0) A, charges N(0, 0.4) e shifted to an integer net charge, seed 0;
   surface from the project's MSMS-format generator at 10 vertices/A^2
-  (~98k faces after the reference's face filter); eps 1/80, 0.15 M; Taylor
+  (92,848 faces after the reference's face filter); eps 1/80, 0.15 M; Taylor
   order 3, MAC 0.8, leaf 500; GMRES tol 1e-4 (MAXL 10, NRMAX 10); FP64.
   The step runs form_matrix -> tree -> interaction lists -> leaf-block LU ->
   GMRES -> solvation energy on device-resident inputs (tabi_run_dev).
@@ -623,7 +623,7 @@ def main():
     ap.add_argument("--batch-workers", type=int, default=4)
     ap.add_argument("--no-large", dest="large", action="store_false",
                     help="skip the large mixed-precision leg (20,000 atoms, order 6, tol 1e-6)")
-    ap.add_argument("--iters", type=int, default=27,
+    ap.add_argument("--iters", type=int, default=6,
                     help="GMRES iterations used to scale the reference-arm sample")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="globular")
     args = ap.parse_args()
