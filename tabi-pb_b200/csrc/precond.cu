@@ -15,6 +15,7 @@
 // (right-looking LU with partial pivoting, the same pivot rule, batched over
 // all leaves) and every apply is a blocked forward/back substitution.
 #include <algorithm>
+#include <climits>
 
 #include "bie_kernels.cuh"
 #include "tabi_impl.cuh"
@@ -457,6 +458,258 @@ __global__ void __launch_bounds__(kPT) lu_panel_kernel(const int* __restrict__ i
   }
 }
 
+// The same panel step with the panel half held in registers: thread t owns
+// the local rows t + NT q (q < R), all 16 columns of the half.  Per column a
+// single CTA barrier: before it, every warp publishes its best candidate
+// (|value|, row) and that row's 16 values, and the owner of the diagonal row
+// publishes it; after it, every warp reduces the candidates itself, takes the
+// winner's row as the pivot row, and each thread swaps, scales and updates its
+// own rows.  Candidates are double-buffered by step parity, so a fast warp's
+// writes of step j+1 cannot meet a slow warp's reads of step j.  The column
+// in work is always register 0: after each step a thread rotates its rows'
+// 16 registers left by one, so the column loop needs no unrolling (an
+// unrolled loop overflowed the instruction cache) and after 16 steps the
+// registers are back in column order.  The operations and their order equal
+// lu_panel_kernel's, so the factors are the same bit for bit.
+constexpr int kRegMaxRows = 2;  // rows per thread of the register panel
+
+struct PanelShared {
+  static constexpr int kMaxW = 16;
+  double cand[2][kMaxW][kSP];  // each warp's best row (rotated order)
+  double cv[2][kMaxW];         // its |value|
+  int ci[2][kMaxW];            // its local row
+  double lrow[2][kSP];         // the diagonal row before the swap
+  int piv[kBP];                // local pivot rows of the panel's columns
+  double u12[kSP][kSP + 1];    // second half: U12 after the TRSM
+};
+
+template <int NT, int R>
+__device__ __forceinline__ void panel_half_reg(double (&a)[R][kSP], int mr, int rbase, int nbh,
+                                               int k0, int& st, int* ip, int* info, int leaf,
+                                               PanelShared& S) {
+  constexpr int NW = NT / 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+#pragma unroll 1
+  for (int j = 0; j < kSP; ++j) {  // nbh pivot steps, then rotations only
+    if (j < nbh) {                 // uniform over the CTA
+      const int lr0 = rbase + j, b = st & 1, rem = nbh - j;
+      double bv = -1.0;
+      int bi = INT_MAX;
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int r = tid + NT * q;
+        if (r >= lr0 && r < mr) argmax_merge(bv, bi, fabs(a[q][0]), r);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        argmax_merge(bv, bi, v2, i2);
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int r = tid + NT * q;
+        if (r == bi) {
+#pragma unroll
+          for (int c = 0; c < kSP; ++c) S.cand[b][warp][c] = a[q][c];
+        }
+        if (r == lr0) {
+#pragma unroll
+          for (int c = 0; c < kSP; ++c) S.lrow[b][c] = a[q][c];
+        }
+      }
+      if (lane == 0) {
+        S.cv[b][warp] = bv;
+        S.ci[b][warp] = bi;
+      }
+      __syncthreads();
+      double v = lane < NW ? S.cv[b][lane] : -1.0;
+      int p = lane < NW ? S.ci[b][lane] : INT_MAX;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, p, o);
+        argmax_merge(v, p, v2, i2);
+      }
+      // no candidate at all (a column of NaNs): keep the diagonal row
+      const double* urow = p == INT_MAX ? S.lrow[b] : S.cand[b][(p % NT) >> 5];
+      if (p == INT_MAX) p = lr0;
+      const double pv = urow[0];
+      if (pv == 0.0) p = lr0;  // a zero column: no interchange
+      if (tid == 0) {
+        S.piv[lr0] = p;
+        ip[k0 + lr0] = k0 + p + 1;  // 1-based, like LAPACK
+      }
+      if (pv != 0.0) {
+        const bool recip = fabs(pv) >= 2.2250738585072014e-308;
+        const double rcp = 1.0 / pv;
+#pragma unroll
+        for (int q = 0; q < R; ++q) {
+          const int r = tid + NT * q;
+          if (p != lr0) {
+            if (r == p) {
+#pragma unroll
+              for (int c = 0; c < kSP; ++c) a[q][c] = S.lrow[b][c];
+            } else if (r == lr0) {
+#pragma unroll
+              for (int c = 0; c < kSP; ++c) a[q][c] = urow[c];
+            }
+          }
+          if (r > lr0 && r < mr) {
+            const double l = recip ? a[q][0] * rcp : a[q][0] / pv;
+            a[q][0] = l;
+#pragma unroll
+            for (int c = 1; c < kSP; ++c)
+              if (c < rem) a[q][c] = fma(-l, urow[c], a[q][c]);
+          }
+        }
+      } else if (tid == 0) {  // DGETRF2: INFO set, no swap, no scaling
+        atomicCAS(&info[leaf], 0, k0 + lr0 + 1);
+      }
+      ++st;
+    }
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const double t0 = a[q][0];
+#pragma unroll
+      for (int c = 0; c < kSP - 1; ++c) a[q][c] = a[q][c + 1];
+      a[q][kSP - 1] = t0;
+    }
+  }
+}
+
+// Source row of local row r after the row interchanges (j, piv[j]) for
+// j = j0 .. j1-1 were applied in order: the swaps replayed backwards.
+__device__ __forceinline__ int swapped_source(int r, const int* piv, int j0, int j1) {
+  for (int j = j1 - 1; j >= j0; --j) {
+    const int pj = piv[j];
+    if (r == j) r = pj;
+    else if (r == pj) r = j;
+  }
+  return r;
+}
+
+template <int NT, int R>
+__global__ void __launch_bounds__(NT, 512 / NT) lu_panel_reg_kernel(
+    const int* __restrict__ items, int k0, const int2* __restrict__ leaf_rng,
+    const int64_t* __restrict__ blk_off, double* __restrict__ lu, int* __restrict__ piv,
+    int* __restrict__ info) {
+  static_assert(NT / 32 <= PanelShared::kMaxW, "too many warps");
+  __shared__ PanelShared S;
+  const int leaf = items[blockIdx.x];
+  const int2 lr = leaf_rng[leaf];
+  const int m = 2 * lr.y;
+  const int nb = min(kBP, m - k0), mr = m - k0;
+  const int nb1 = min(kSP, nb), nb2 = nb - nb1;
+  double* A = lu + blk_off[leaf];
+  int* ip = piv + 2 * lr.x;
+  const int tid = threadIdx.x;
+  int st = 0;
+  double a[R][kSP];
+#pragma unroll 1
+  for (int h = 0; h < 2; ++h) {  // the two 16-column halves
+    const int nbh = h == 0 ? nb1 : nb2, cb = k0 + kSP * h;
+    if (nbh == 0) break;
+    if (h == 0) {
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int r = tid + NT * q;
+#pragma unroll
+        for (int c = 0; c < kSP; ++c)
+          a[q][c] = (r < mr && c < nb1) ? A[(size_t)(k0 + c) * m + k0 + r] : 0.0;
+      }
+    } else {
+      // load through the first half's swaps, TRSM, GEMM update
+      __syncthreads();  // pivots and the stored first half visible to all
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int r = tid + NT * q;
+        const int src = r < mr ? swapped_source(r, S.piv, 0, kSP) : r;
+#pragma unroll
+        for (int c = 0; c < kSP; ++c)
+          a[q][c] = (r < mr && c < nb2) ? A[(size_t)(cb + c) * m + k0 + src] : 0.0;
+      }
+      if (tid < 32) {  // U12 = L11^{-1} A12: rows 0..15 are lanes 0..15, q = 0
+        const int lane = tid;
+        double l11[kSP];
+#pragma unroll
+        for (int q = 0; q < kSP; ++q)
+          l11[q] = lane < kSP ? A[(size_t)(k0 + q) * m + k0 + lane] : 0.0;
+#pragma unroll
+        for (int q = 0; q < kSP - 1; ++q)
+#pragma unroll
+          for (int c = 0; c < kSP; ++c) {
+            const double x = __shfl_sync(0xffffffffu, a[0][c], q);
+            if (lane > q && lane < kSP) a[0][c] = fma(-l11[q], x, a[0][c]);
+          }
+        if (lane < kSP)
+#pragma unroll
+          for (int c = 0; c < kSP; ++c) S.u12[lane][c] = a[0][c];
+      }
+      __syncthreads();
+#pragma unroll
+      for (int q = 0; q < R; ++q) {  // rows 16.. -= L21 U12 (per element k = 0..15 in order)
+        const int r = tid + NT * q;
+        if (r >= kSP && r < mr) {
+          const double* lrow = A + (size_t)k0 * m + k0 + r;
+#pragma unroll 1
+          for (int k = 0; k < kSP; ++k) {
+            const double l = lrow[(size_t)k * m];
+#pragma unroll
+            for (int c = 0; c < kSP; ++c) a[q][c] = fma(-l, S.u12[k][c], a[q][c]);
+          }
+        }
+      }
+    }
+    panel_half_reg<NT, R>(a, mr, kSP * h, nbh, k0, st, ip, info, leaf, S);
+#pragma unroll
+    for (int q = 0; q < R; ++q) {
+      const int r = tid + NT * q;
+      if (r < mr) {
+#pragma unroll
+        for (int c = 0; c < kSP; ++c)
+          if (c < nbh) A[(size_t)(cb + c) * m + k0 + r] = a[q][c];
+      }
+    }
+  }
+  if (nb2 == 0) return;
+  __syncthreads();
+  // the second half's swaps on the first half's columns: slot s < 16 is the
+  // diagonal row 16 + s, slot 16 + j the pivot row of column 16 + j when it is
+  // below the panel's diagonal rows and not named by an earlier column
+  constexpr int kPer = (2 * kSP * kSP + NT - 1) / NT;
+  double v[kPer];
+  int dst[kPer];
+#pragma unroll
+  for (int e = 0; e < kPer; ++e) {
+    const int u = tid + NT * e, s = u / kSP, c = u - s * kSP;
+    int t = -1;
+    if (s < kSP) {
+      if (s < nb2) t = kSP + s;
+    } else if (s - kSP < nb2) {
+      const int j = s - kSP, pj = S.piv[kSP + j];
+      t = pj;
+      if (pj < nb) t = -1;
+      for (int j2 = 0; j2 < j; ++j2)
+        if (S.piv[kSP + j2] == pj) t = -1;
+    }
+    dst[e] = -1;
+    if (u < 2 * kSP * kSP && t >= 0) {
+      const int src = swapped_source(t, S.piv, kSP, kSP + nb2);
+      if (src != t) {
+        v[e] = A[(size_t)(k0 + c) * m + k0 + src];
+        dst[e] = t;
+      }
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (int e = 0; e < kPer; ++e) {
+    const int u = tid + NT * e, c = u % kSP;
+    if (dst[e] >= 0) A[(size_t)(k0 + c) * m + k0 + dst[e]] = v[e];
+  }
+}
+
 // item = (leaf, c0, c1, mode): columns [c0, c1) of the leaf block.
 // mode 0: left of the panel, the panel's swaps; 1: right of the panel, the
 // panel's swaps then U12 = L11^{-1} A12; 3: U12 = L11^{-1} A12 only (columns
@@ -548,13 +801,30 @@ __global__ void __launch_bounds__(kUT) lu_strip_kernel(const int4* __restrict__ 
 // at ce, packed as ends = (re << 16) | ce (0: both m).  The C tile is read and
 // written once per launch, so a 128-deep update moves a quarter of the bytes
 // of four 32-deep ones.
-__global__ void __launch_bounds__(kUT) lu_gemm_kernel(const int4* __restrict__ items, int k0,
-                                                      int kdepth,
-                                                      const int2* __restrict__ leaf_rng,
-                                                      const int64_t* __restrict__ blk_off,
-                                                      double* __restrict__ lu) {
-  __shared__ double sL[kBP][kGT + 1];
-  __shared__ double sU[kBP][kGT + 1];
+//
+// The 32-deep slices of L and U are copied into shared memory with cp.async
+// (16-byte chunks, zero-filled outside the tile), double-buffered: slice k+1
+// is in flight while slice k is multiplied.  Every address is 16-byte
+// aligned: blocks start at multiples of 4 doubles, m and all row and column
+// offsets are even, and a slice's depth is even, so a chunk (two doubles) is
+// either wholly inside the tile or wholly outside it.
+constexpr int kUPitch = kBP + 2;  // U slice stored by column, 16-byte aligned rows
+constexpr size_t kGemmSmem = sizeof(double) * 2 * (kBP * kGT + kGT * kUPitch);
+
+__device__ __forceinline__ void cp_async16(double* dst, const double* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src),
+               "r"(valid ? 16 : 0));
+}
+
+__global__ void __launch_bounds__(kUT, 2) lu_gemm_kernel(const int4* __restrict__ items, int k0,
+                                                         int kdepth,
+                                                         const int2* __restrict__ leaf_rng,
+                                                         const int64_t* __restrict__ blk_off,
+                                                         double* __restrict__ lu) {
+  extern __shared__ double gsm[];
+  double* sLb = gsm;                      // [2][kBP][kGT]: L slice, k-major
+  double* sUb = gsm + 2 * kBP * kGT;      // [2][kGT][kUPitch]: U slice, by column
   const int4 it = items[blockIdx.x];
   const int leaf = it.x, r0 = it.y, c0 = it.z;
   const int m = 2 * leaf_rng[leaf].y;
@@ -562,6 +832,28 @@ __global__ void __launch_bounds__(kUT) lu_gemm_kernel(const int4* __restrict__ i
   const int kd = min(kdepth, m - k0);
   double* A = lu + blk_off[leaf];
   const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
+  // issue the copies of the slice starting at column k0 + kc into buffer buf
+  auto load_slice = [&](int kc, int buf) {
+    const int nbk = min(kBP, kd - kc), kb = k0 + kc;
+    double* sL = sLb + buf * kBP * kGT;
+    double* sU = sUb + buf * kGT * kUPitch;
+#pragma unroll
+    for (int e = 0; e < (kBP * kGT / 2) / kUT; ++e) {
+      const int q = tid + kUT * e;
+      const int k = q / (kGT / 2), rr = 2 * (q % (kGT / 2));
+      const bool ok = k < nbk && r0 + rr < re;
+      cp_async16(sL + k * kGT + rr, ok ? A + (size_t)(kb + k) * m + r0 + rr : A, ok);
+    }
+#pragma unroll
+    for (int e = 0; e < (kGT * kBP / 2) / kUT; ++e) {
+      const int q = tid + kUT * e;
+      const int cc = q / (kBP / 2), kk = 2 * (q % (kBP / 2));
+      const bool ok = kk < nbk && c0 + cc < ce;
+      cp_async16(sU + cc * kUPitch + kk, ok ? A + (size_t)(c0 + cc) * m + kb + kk : A, ok);
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  load_slice(0, 0);
   // C values first (independent of the tiles)
   double cv[4][4];
 #pragma unroll
@@ -579,30 +871,29 @@ __global__ void __launch_bounds__(kUT) lu_gemm_kernel(const int4* __restrict__ i
   for (int a = 0; a < 4; ++a)
 #pragma unroll
     for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
-  for (int kc = 0; kc < kd; kc += kBP) {
-    const int nbk = min(kBP, kd - kc), kb = k0 + kc;
-    if (kc > 0) __syncthreads();
-    for (int q = tid; q < kBP * kGT; q += kUT) {
-      int k = q / kGT, rr = q - k * kGT;
-      int r = r0 + rr;
-      sL[k][rr] = (k < nbk && r < re) ? A[(size_t)(kb + k) * m + r] : 0.0;
-      int k2 = q % kBP, cc2 = q / kBP;
-      int c = c0 + cc2;
-      sU[k2][cc2] = (k2 < nbk && c < ce) ? A[(size_t)c * m + kb + k2] : 0.0;
+  for (int kc = 0, buf = 0; kc < kd; kc += kBP, buf ^= 1) {
+    if (kc + kBP < kd) {
+      load_slice(kc + kBP, buf ^ 1);
+      asm volatile("cp.async.wait_group 1;\n" ::);
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::);
     }
     __syncthreads();
+    const double* sL = sLb + buf * kBP * kGT;
+    const double* sU = sUb + buf * kGT * kUPitch;
 #pragma unroll 8
     for (int k = 0; k < kBP; ++k) {
       double lv[4], uv[4];
 #pragma unroll
-      for (int a = 0; a < 4; ++a) lv[a] = sL[k][tr + 16 * a];
+      for (int a = 0; a < 4; ++a) lv[a] = sL[k * kGT + tr + 16 * a];
 #pragma unroll
-      for (int b = 0; b < 4; ++b) uv[b] = sU[k][tc + 16 * b];
+      for (int b = 0; b < 4; ++b) uv[b] = sU[(tc + 16 * b) * kUPitch + k];
 #pragma unroll
       for (int a = 0; a < 4; ++a)
 #pragma unroll
         for (int b = 0; b < 4; ++b) acc[a][b] = fma(lv[a], uv[b], acc[a][b]);
     }
+    __syncthreads();  // buffer buf is refilled two slices on
   }
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
@@ -1022,6 +1313,7 @@ void build_precond(Handle& H, cudaStream_t s) {
       size_t smem = sizeof(double) * (size_t)mmax * kSP;
       raise_smem_limit((const void*)lu_panel_kernel, std::max<size_t>(smem, 48 * 1024));
     }
+    raise_smem_limit((const void*)lu_gemm_kernel, kGemmSmem);
     for (const Launch& L : plan) {
       switch (L.kind) {
         case 0: {
@@ -1035,21 +1327,27 @@ void build_precond(Handle& H, cudaStream_t s) {
             TABI_CUDA(cudaEventRecord(H.ev_fork, s));
             TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
           }
-          if (nbig > 0) {
-            const int mr = 2 * rng[pitems[L.off]].y - L.k0;
-            TABI_K(K_LU, s);
-            lu_panel_kernel<<<nbig, kPT, sizeof(double) * (size_t)mr * kSP, s>>>(
-                H.pc_list.p + L.off, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
-                d_info.p);
-          }
-          if (nbig < L.cnt) {
-            cudaStream_t s2 = fork ? H.side : s;
-            const int mr = 2 * rng[pitems[L.off + nbig]].y - L.k0;
-            TABI_K(K_LU, s2);
-            lu_panel_kernel<<<L.cnt - nbig, kPT, sizeof(double) * (size_t)mr * kSP, s2>>>(
-                H.pc_list.p + L.off + nbig, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p,
-                T.d_piv.p, d_info.p);
-          }
+          // the register-resident panel up to 512 x kRegMaxRows rows left, the
+          // shared-memory one above
+          auto panel = [&](int cnt, const int* list, int mr, cudaStream_t st) {
+            TABI_K(K_LU, st);
+            if (mr <= 256)
+              lu_panel_reg_kernel<256, 1><<<cnt, 256, 0, st>>>(
+                  list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
+            else if (mr <= 512)
+              lu_panel_reg_kernel<512, 1><<<cnt, 512, 0, st>>>(
+                  list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
+            else if (mr <= 512 * kRegMaxRows)
+              lu_panel_reg_kernel<512, kRegMaxRows><<<cnt, 512, 0, st>>>(
+                  list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
+            else
+              lu_panel_kernel<<<cnt, kPT, sizeof(double) * (size_t)mr * kSP, st>>>(
+                  list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
+          };
+          if (nbig > 0) panel(nbig, H.pc_list.p + L.off, 2 * rng[pitems[L.off]].y - L.k0, s);
+          if (nbig < L.cnt)
+            panel(L.cnt - nbig, H.pc_list.p + L.off + nbig,
+                  2 * rng[pitems[L.off + nbig]].y - L.k0, fork ? H.side : s);
           if (fork) {
             TABI_CUDA(cudaEventRecord(H.ev_join, H.side));
             TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
@@ -1064,8 +1362,8 @@ void build_precond(Handle& H, cudaStream_t s) {
         }
         case 2: {
           TABI_K(K_LU_UPDATE, s);
-          lu_gemm_kernel<<<L.cnt, kUT, 0, s>>>(H.pc_gitems.p + L.off, L.k0, L.kdepth,
-                                               T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p);
+          lu_gemm_kernel<<<L.cnt, kUT, kGemmSmem, s>>>(H.pc_gitems.p + L.off, L.k0, L.kdepth,
+                                                       T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p);
           break;
         }
         case 3: {
