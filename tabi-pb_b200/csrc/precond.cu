@@ -468,150 +468,115 @@ __global__ void __launch_bounds__(kPT) lu_panel_kernel(const int* __restrict__ i
 // publishes it; after it, every warp reduces the candidates itself, takes the
 // winner's row as the pivot row, and each thread swaps, scales and updates its
 // own rows.  Candidates are double-buffered by step parity, so a fast warp's
-// writes of step j+1 cannot meet a slow warp's reads of step j.  Columns are
-// taken in groups of four at fixed register positions 0..3: after each group
-// a thread rotates its rows' 16 registers left by four, so only one group is
-// unrolled (a fully unrolled column loop overflowed the instruction cache) and
-// after four groups the registers are back in column order.  The operations and their order equal
+// writes of step j+1 cannot meet a slow warp's reads of step j.  The column
+// in work is always register 0: after each step a thread rotates its rows'
+// 16 registers left by one, so the column loop needs no unrolling (an
+// unrolled loop overflowed the instruction cache) and after 16 steps the
+// registers are back in column order.  The operations and their order equal
 // lu_panel_kernel's, so the factors are the same bit for bit.
 constexpr int kRegMaxRows = 2;  // rows per thread of the register panel
 
-struct __align__(16) PanelShared {
+struct PanelShared {
   static constexpr int kMaxW = 16;
   double cand[2][kMaxW][kSP];  // each warp's best row (rotated order)
-  double lrow[2][kSP];         // the diagonal row before the swap
-  double u12[kSP][kSP + 1];    // second half: U12 after the TRSM
-  double cv[2][kMaxW];         // each warp's best |value|
+  double cv[2][kMaxW];         // its |value|
   int ci[2][kMaxW];            // its local row
+  double lrow[2][kSP];         // the diagonal row before the swap
   int piv[kBP];                // local pivot rows of the panel's columns
+  double u12[kSP][kSP + 1];    // second half: U12 after the TRSM
 };
-
-// Largest |value| of the lanes, then the smallest row among the lanes that
-// hold it (IDAMAX's first index on ties); lanes without a candidate hold
-// (-1, INT_MAX).  Returns the row; every lane gets the same answer.
-__device__ __forceinline__ int warp_argmax(double v, int i, double* vmax) {
-  double m = v;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-  *vmax = m;
-  return (int)__reduce_min_sync(0xffffffffu, v == m ? (unsigned)i : (unsigned)INT_MAX);
-}
-
-__device__ __forceinline__ void store_row(double* dst, const double (&row)[kSP]) {
-#pragma unroll
-  for (int c = 0; c < kSP; c += 2)
-    *reinterpret_cast<double2*>(dst + c) = make_double2(row[c], row[c + 1]);
-}
-
-__device__ __forceinline__ void load_row(double (&row)[kSP], const double* src) {
-#pragma unroll
-  for (int c = 0; c < kSP; c += 2) {
-    const double2 t = *reinterpret_cast<const double2*>(src + c);
-    row[c] = t.x;
-    row[c + 1] = t.y;
-  }
-}
 
 template <int NT, int R>
 __device__ __forceinline__ void panel_half_reg(double (&a)[R][kSP], int mr, int rbase, int nbh,
                                                int k0, int& st, int* ip, int* info, int leaf,
                                                PanelShared& S) {
   constexpr int NW = NT / 32;
-  constexpr int kG = 4;  // columns per rotation
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
 #pragma unroll 1
-  for (int jj = 0; jj < kSP; jj += kG) {
+  for (int j = 0; j < kSP; ++j) {  // nbh pivot steps, then rotations only
+    if (j < nbh) {                 // uniform over the CTA
+      const int lr0 = rbase + j, b = st & 1, rem = nbh - j;
+      double bv = -1.0;
+      int bi = INT_MAX;
 #pragma unroll
-    for (int j4 = 0; j4 < kG; ++j4) {
-      const int j = jj + j4;
-      if (j < nbh) {  // uniform over the CTA
-        const int lr0 = rbase + j, b = st & 1, cend = nbh - jj;
-        double bv = -1.0;
-        int bi = INT_MAX;
+      for (int q = 0; q < R; ++q) {
+        const int r = tid + NT * q;
+        if (r >= lr0 && r < mr) argmax_merge(bv, bi, fabs(a[q][0]), r);
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, bi, o);
+        argmax_merge(bv, bi, v2, i2);
+      }
+#pragma unroll
+      for (int q = 0; q < R; ++q) {
+        const int r = tid + NT * q;
+        if (r == bi) {
+#pragma unroll
+          for (int c = 0; c < kSP; ++c) S.cand[b][warp][c] = a[q][c];
+        }
+        if (r == lr0) {
+#pragma unroll
+          for (int c = 0; c < kSP; ++c) S.lrow[b][c] = a[q][c];
+        }
+      }
+      if (lane == 0) {
+        S.cv[b][warp] = bv;
+        S.ci[b][warp] = bi;
+      }
+      __syncthreads();
+      double v = lane < NW ? S.cv[b][lane] : -1.0;
+      int p = lane < NW ? S.ci[b][lane] : INT_MAX;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        const double v2 = __shfl_xor_sync(0xffffffffu, v, o);
+        const int i2 = __shfl_xor_sync(0xffffffffu, p, o);
+        argmax_merge(v, p, v2, i2);
+      }
+      // no candidate at all (a column of NaNs): keep the diagonal row
+      const double* urow = p == INT_MAX ? S.lrow[b] : S.cand[b][(p % NT) >> 5];
+      if (p == INT_MAX) p = lr0;
+      const double pv = urow[0];
+      if (pv == 0.0) p = lr0;  // a zero column: no interchange
+      if (tid == 0) {
+        S.piv[lr0] = p;
+        ip[k0 + lr0] = k0 + p + 1;  // 1-based, like LAPACK
+      }
+      if (pv != 0.0) {
+        const bool recip = fabs(pv) >= 2.2250738585072014e-308;
+        const double rcp = 1.0 / pv;
 #pragma unroll
         for (int q = 0; q < R; ++q) {
           const int r = tid + NT * q;
-          if (r >= lr0 && r < mr) argmax_merge(bv, bi, fabs(a[q][j4]), r);
-        }
-        double wv;
-        const int wi = warp_argmax(bv, bi, &wv);
+          if (p != lr0) {
+            if (r == p) {
 #pragma unroll
-        for (int q = 0; q < R; ++q)
-          if (tid + NT * q == wi) store_row(S.cand[b][warp], a[q]);
-        if (warp == (lr0 % NT) >> 5) {
+              for (int c = 0; c < kSP; ++c) a[q][c] = S.lrow[b][c];
+            } else if (r == lr0) {
 #pragma unroll
-          for (int q = 0; q < R; ++q)
-            if (tid + NT * q == lr0) store_row(S.lrow[b], a[q]);
-        }
-        if (lane == 0) {
-          S.cv[b][warp] = wv;
-          S.ci[b][warp] = wi;
-        }
-        __syncthreads();
-        double pvmax;
-        int p = warp_argmax(lane < NW ? S.cv[b][lane] : -1.0,
-                            lane < NW ? S.ci[b][lane] : INT_MAX, &pvmax);
-        // no candidate at all (a column of NaNs): keep the diagonal row
-        const double* urow = p == INT_MAX ? S.lrow[b] : S.cand[b][(p % NT) >> 5];
-        if (p == INT_MAX) p = lr0;
-        const double pv = urow[j4];
-        if (pv == 0.0) p = lr0;  // a zero column: no interchange
-        if (tid == 0) {
-          S.piv[lr0] = p;
-          ip[k0 + lr0] = k0 + p + 1;  // 1-based, like LAPACK
-        }
-        if (pv != 0.0) {
-          if (p != lr0 && (warp == (p % NT) >> 5 || warp == (lr0 % NT) >> 5)) {
-#pragma unroll
-            for (int q = 0; q < R; ++q) {
-              const int r = tid + NT * q;
-              if (r == p) load_row(a[q], S.lrow[b]);
-              else if (r == lr0) load_row(a[q], urow);
+              for (int c = 0; c < kSP; ++c) a[q][c] = urow[c];
             }
           }
-          const bool recip = fabs(pv) >= 2.2250738585072014e-308;  // uniform
-          const double rcp = 1.0 / pv;
-          double l[R];
-          if (recip) {
+          if (r > lr0 && r < mr) {
+            const double l = recip ? a[q][0] * rcp : a[q][0] / pv;
+            a[q][0] = l;
 #pragma unroll
-            for (int q = 0; q < R; ++q) l[q] = a[q][j4] * rcp;
-          } else {
-#pragma unroll
-            for (int q = 0; q < R; ++q) l[q] = a[q][j4] / pv;
+            for (int c = 1; c < kSP; ++c)
+              if (c < rem) a[q][c] = fma(-l, urow[c], a[q][c]);
           }
-          bool mine[R];
-#pragma unroll
-          for (int q = 0; q < R; ++q) {
-            const int r = tid + NT * q;
-            mine[q] = r > lr0 && r < mr;
-            if (mine[q]) a[q][j4] = l[q];
-          }
-#pragma unroll
-          for (int cp = 0; cp < kSP / 2; ++cp) {
-            if (2 * cp + 1 <= j4) continue;
-            const double2 u = *reinterpret_cast<const double2*>(urow + 2 * cp);
-#pragma unroll
-            for (int q = 0; q < R; ++q) {
-              if (!mine[q]) continue;
-              if (2 * cp > j4 && 2 * cp < cend) a[q][2 * cp] = fma(-l[q], u.x, a[q][2 * cp]);
-              if (2 * cp + 1 < cend) a[q][2 * cp + 1] = fma(-l[q], u.y, a[q][2 * cp + 1]);
-            }
-          }
-        } else if (tid == 0) {  // DGETRF2: INFO set, no swap, no scaling
-          atomicCAS(&info[leaf], 0, k0 + lr0 + 1);
         }
-        ++st;
+      } else if (tid == 0) {  // DGETRF2: INFO set, no swap, no scaling
+        atomicCAS(&info[leaf], 0, k0 + lr0 + 1);
       }
+      ++st;
     }
 #pragma unroll
     for (int q = 0; q < R; ++q) {
-      double t[kG];
+      const double t0 = a[q][0];
 #pragma unroll
-      for (int c = 0; c < kG; ++c) t[c] = a[q][c];
-#pragma unroll
-      for (int c = 0; c < kSP - kG; ++c) a[q][c] = a[q][c + kG];
-#pragma unroll
-      for (int c = 0; c < kG; ++c) a[q][kSP - kG + c] = t[c];
+      for (int c = 0; c < kSP - 1; ++c) a[q][c] = a[q][c + 1];
+      a[q][kSP - 1] = t0;
     }
   }
 }
