@@ -54,6 +54,7 @@ WORKLOAD_ITERS = None
 # trained warm-start network (tabipb.train_warmstart)
 WEIGHTS = os.path.join(ROOT, "tabi-pb_b200", "weights", "warmstart_h160_l3.npz")
 OPS_NEAR_PAIR = 64  # algorithmic ops per near-field pair (reference formulas)
+REF_BUDGET_S = 150.0  # wall-clock bound of the reference arm's timed steps
 
 
 def far_ops(p):
@@ -91,10 +92,16 @@ class Clocks:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # sampling has begun once the first line is in; samples taken
+            # before the timed region are dropped
+            t0 = time.time()
+            while not self.lines and time.time() - t0 < 5.0:
+                time.sleep(0.01)
+            self.lines.clear()
         except Exception:
             self.proc = None
 
@@ -586,11 +593,20 @@ def reference_arm(args):
     for _ in range(args.warmup):
         oracle_estimate(inp, iters, nthreads, target_sample=2048, leaf_sample=4, atom_sample=16,
                         face_frac=0.05)
+    # the first timed step takes the full sample; later steps shrink theirs so
+    # that all steps together stay within about REF_BUDGET_S seconds
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        v, parts, sample = oracle_estimate(inp, iters, nthreads, target_sample=65536,
-                                           leaf_sample=10 ** 9, atom_sample=400)
+    scale = 1.0
+    for k in range(args.steps):
+        ts = time.perf_counter()
+        v, parts, sample = oracle_estimate(
+            inp, iters, nthreads, target_sample=max(2048, int(65536 * scale)),
+            leaf_sample=10 ** 9 if scale >= 1.0 else max(4, int(600 * scale)),
+            atom_sample=max(16, int(400 * scale)))
         vals.append(v)
+        if k == 0 and args.steps > 1:
+            w1 = time.perf_counter() - ts
+            scale = min(1.0, max(0.02, (REF_BUDGET_S - w1) / ((args.steps - 1) * w1)))
     wall = time.perf_counter() - t0
     value = float(np.mean(vals))
     print(json.dumps({
@@ -612,7 +628,7 @@ def reference_arm(args):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=30)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=("gpu", "reference"), default="gpu")
     ap.add_argument("--no-cpu-baseline", action="store_true")
