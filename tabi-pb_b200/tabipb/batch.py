@@ -97,3 +97,20 @@ def autotune(probes, params, candidates=(200, 300, 400, 500, 700), repeats=2, lo
                 best = (t, leaf)
         table[c] = best[1]
     return table, timings
+
+
+def tune_workers(mols, params, table, candidates=(1, 2, 4), ws=None, repeats=2):
+    """Times the batch call on `mols` for each worker count and returns the
+    fastest count and the timings {workers: s}.  Concurrency pays when one
+    molecule's launches leave the GPU idle (host round trips, short launch
+    chains); when each solve already fills the GPU, extra workers only
+    contend, so the count is measured, not assumed."""
+    timings = {}
+    for nw in candidates:
+        ts = []
+        for _ in range(repeats):
+            _, t = run_batch(mols, params, ws=ws, nworkers=nw, table=table)
+            ts.append(t)
+        timings[nw] = min(ts)
+    best = min(timings, key=timings.get)
+    return best, timings

@@ -92,3 +92,16 @@ def test_autotune_picks_a_candidate(mols):
     c = B.size_class(mols[4]["nface"])
     assert table[c] in (150, 300)
     assert timings[(c, table[c])] == min(timings[(c, 150)], timings[(c, 300)])
+
+
+def test_worker_tuner_picks_the_fastest_count(mols):
+    from tabipb import batch as B
+
+    prm = _params(precision=1, maxparnode=300)
+    nw, timings = B.tune_workers(mols, prm, None, candidates=(1, 2), repeats=1)
+    assert set(timings) == {1, 2} and nw in (1, 2)
+    assert timings[nw] == min(timings.values())
+    # the chosen count changes nothing but the overlap
+    a, _ = B.run_batch(mols, prm, nworkers=1)
+    b, _ = B.run_batch(mols, prm, nworkers=nw)
+    assert np.array_equal(a[:, 3], b[:, 3]) and np.array_equal(a[:, 0], b[:, 0])
