@@ -525,7 +525,7 @@ def batched_leg(args, dev, rank):
     benchmark's atom density and surface density, mixed precision, tol 1e-4,
     leaf size per size class from the autotuner, the trained warm start when
     its weights exist, and the worker count (1, 2 or --batch-workers) that
-    ran the first half of the batch fastest.  Reported: molecules/s of the
+    ran the first quarter of the batch fastest.  Reported: molecules/s of the
     whole batch on that many workers and on one (the same molecules back to
     back), and the per-molecule wall-time percentiles."""
     import multiprocessing as mp
@@ -562,9 +562,9 @@ def batched_leg(args, dev, rank):
 
         ws = WarmStart.load(WEIGHTS)
     B.run_batch(mols[:2], prm, ws=ws, nworkers=2, table=table)  # warm-up
-    # worker count: measured on the first half of the batch
+    # worker count: measured on the first quarter of the batch (at least 8)
     cands = tuple(sorted({1, 2, args.batch_workers}))
-    nw, wt = B.tune_workers(mols[: max(2, len(mols) // 2)], prm, table, candidates=cands, ws=ws,
+    nw, wt = B.tune_workers(mols[: max(8, len(mols) // 4)], prm, table, candidates=cands, ws=ws,
                             repeats=2)
 
     def best_of(n, nworkers):  # the batch call's wall time varies run to run
@@ -645,7 +645,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true",
                     help="skip the mixed-precision leg (FP32 treecode + FP64 refinement)")
-    ap.add_argument("--batch", type=int, default=16,
+    ap.add_argument("--batch", type=int, default=256,
                     help="molecules in the batched leg (0 skips it)")
     ap.add_argument("--batch-workers", type=int, default=4)
     ap.add_argument("--no-large", dest="large", action="store_false",
