@@ -1108,51 +1108,80 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     if (kp + lane < m) prefetch_l2(A + (size_t)(kp + lane) * m, kp);
     if (lane == 0) prefetch_l2(Di + (size_t)bp * 2 * kDB * kDB + kDB * kDB, kDB * kDB);
   };
-  // step: y = Dinv * run[k0 .. k0+nb) (all warps), res[k0 ..] = y (warp 0),
-  // run[i] -= A[i, k0 .. k0+nb) y for the rows [i0, i1)
-  auto step = [&](int k0, int nb, const double* Dblk, double* run, double* res, int i0,
-                  int i1) {
-    double v = 0.0;
+  // the inverse diagonal block of sweep step t (L blocks 0..nblk-1, then U
+  // blocks nblk-1..0), staged into shared memory one step ahead by cp.async
+  const int nblk = (m + kDB - 1) / kDB;
+  double* dbuf = ys + 32 * (NT / 32);  // [2][kDB * kDB]
+  auto stage = [&](int t, int buf) {
+    if (t >= 2 * nblk) return;
+    const int b = t < nblk ? t : 2 * nblk - 1 - t;
+    const double* src = Di + (size_t)b * 2 * kDB * kDB + (t < nblk ? 0 : kDB * kDB);
+    for (int e = 2 * tid; e < kDB * kDB; e += 2 * NT) {
+      const unsigned d = (unsigned)__cvta_generic_to_shared(dbuf + buf * kDB * kDB + e);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + e));
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  // step t: y = Dinv * run[k0 .. k0+nb) (all warps), res[k0 ..] = y (warp 0),
+  // run[i] -= A[i, k0 .. k0+nb) y for the rows [i0, i1); the next step's block
+  // is copied while the rows are updated.  Four partial sums per dot product
+  // keep the dependent FMA chains 8 deep.
+  auto step = [&](int t, int k0, int nb, double* run, double* res, int i0, int i1) {
+    const double* Dblk = dbuf + (t & 1) * kDB * kDB;
+    double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
 #pragma unroll
-    for (int q = 0; q < kDB; ++q)
-      if (q < nb) v = fma(Dblk[(size_t)q * kDB + lane], run[k0 + q], v);
+    for (int q = 0; q < kDB; q += 4) {
+      if (q < nb) v0 = fma(Dblk[q * kDB + lane], run[k0 + q], v0);
+      if (q + 1 < nb) v1 = fma(Dblk[(q + 1) * kDB + lane], run[k0 + q + 1], v1);
+      if (q + 2 < nb) v2 = fma(Dblk[(q + 2) * kDB + lane], run[k0 + q + 2], v2);
+      if (q + 3 < nb) v3 = fma(Dblk[(q + 3) * kDB + lane], run[k0 + q + 3], v3);
+    }
+    const double v = (v0 + v1) + (v2 + v3);
     yw[lane] = v;
     if (warp == 0 && lane < nb) res[k0 + lane] = v;
     __syncwarp();
+    stage(t + 1, (t + 1) & 1);
     for (int i = i0 + tid; i < i1; i += NT) {
       const double* a = A + (size_t)k0 * m + i;
-      double s = run[i];
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
       if (nb == kDB) {
-        double t[kDB];
+        double tq[kDB];
 #pragma unroll
-        for (int q = 0; q < kDB; ++q) t[q] = a[(size_t)q * m];
+        for (int q = 0; q < kDB; ++q) tq[q] = a[(size_t)q * m];
 #pragma unroll
-        for (int q = 0; q < kDB; ++q) s = fma(-t[q], yw[q], s);
+        for (int q = 0; q < kDB; q += 4) {
+          s0 = fma(tq[q], yw[q], s0);
+          s1 = fma(tq[q + 1], yw[q + 1], s1);
+          s2 = fma(tq[q + 2], yw[q + 2], s2);
+          s3 = fma(tq[q + 3], yw[q + 3], s3);
+        }
       } else {
-        for (int q = 0; q < nb; ++q) s = fma(-a[(size_t)q * m], yw[q], s);
+        for (int q = 0; q < nb; ++q) s0 = fma(a[(size_t)q * m], yw[q], s0);
       }
-      run[i] = s;
+      run[i] -= (s0 + s1) + (s2 + s3);
     }
+    asm volatile("cp.async.wait_group 0;\n" ::);
     __syncthreads();
   };
   if (warp == 1)
     for (int q = 0; q < kPF; ++q) pf_lower(q * kDB);
+  stage(0, 0);
+  asm volatile("cp.async.wait_group 0;\n" ::);
   __syncthreads();
   // L y = P r: running values in xs, y in fin
-  for (int k0 = 0; k0 < m; k0 += kDB) {
+  for (int k0 = 0, t = 0; k0 < m; k0 += kDB, ++t) {
     const int nb = min(kDB, m - k0);
     if (warp == 1) pf_lower(k0 + kPF * kDB);
-    step(k0, nb, Di + (size_t)(k0 / kDB) * 2 * kDB * kDB, xs, fin, k0 + nb, m);
+    step(t, k0, nb, xs, fin, k0 + nb, m);
   }
   // U x = y: running values in fin, x in xs
-  const int nblk = (m + kDB - 1) / kDB;
   if (warp == 1)
     for (int q = 0; q < kPF; ++q) pf_upper(nblk - 1 - q);
-  for (int b = nblk - 1; b >= 0; --b) {
+  for (int b = nblk - 1, t = nblk; b >= 0; --b, ++t) {
     const int k0 = b * kDB;
     const int nb = min(kDB, m - k0);
     if (warp == 1) pf_upper(b - kPF);
-    step(k0, nb, Di + (size_t)b * 2 * kDB * kDB + kDB * kDB, fin, xs, 0, k0);
+    step(t, k0, nb, fin, xs, 0, k0);
   }
   for (int i = tid; i < n; i += NT) {
     z[ib + i] = xs[i];
@@ -1450,8 +1479,9 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
     TABI_CUDA(cudaGetLastError());
     return;
   }
-  // two arrays of the block order m = 2 * leaf size, plus 32 doubles per warp
-  size_t smem = sizeof(double) * (4 * (size_t)T.max_leaf + 512);
+  // two arrays of the block order m = 2 * leaf size, 32 doubles per warp and
+  // two staged 32 x 32 inverse diagonal blocks
+  size_t smem = sizeof(double) * (4 * (size_t)T.max_leaf + 512 + 2 * kDB * kDB);
   TABI_REQUIRE(smem <= 200 * 1024, TABI_ERR_LIMIT, "leaf too large for the block solve");
   if (smem > 48 * 1024) {
     raise_smem_limit((const void*)solve_kernel<256>, smem);
