@@ -1089,7 +1089,6 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
   const double* Di = dinv + dinv_off[leaf];
   const int* pm = perm + 2 * ib;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  double* yw = ys + 32 * warp;
   for (int i = tid; i < m; i += NT) {
     int src = pm[i];
     xs[i] = (src < n) ? r[ib + src] : r[N + ib + src - n];
@@ -1122,43 +1121,83 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     }
     asm volatile("cp.async.commit_group;\n" ::);
   };
-  // step t: y = Dinv * run[k0 .. k0+nb) (all warps), res[k0 ..] = y (warp 0),
-  // run[i] -= A[i, k0 .. k0+nb) y for the rows [i0, i1); the next step's block
-  // is copied while the rows are updated.  Four partial sums per dot product
-  // keep the dependent FMA chains 8 deep.
-  auto step = [&](int t, int k0, int nb, double* run, double* res, int i0, int i1) {
+  // step t: y = Dinv * run[k0 .. k0+nb), res[k0 ..] = y, run[i] -= A[i, k0 ..
+  // k0+nb) y for the rows [i0, i1); the next step's block is copied while the
+  // rows are updated.  Four partial sums per dot product keep the dependent
+  // FMA chains 8 deep.
+  // y = Dinv * run[k0 .. k0+nb) for lane `lane`, four partial sums
+  auto diag = [&](int t, int k0, int nb, const double* run) {
     const double* Dblk = dbuf + (t & 1) * kDB * kDB;
     double v0 = 0.0, v1 = 0.0, v2 = 0.0, v3 = 0.0;
+    if (nb == kDB) {  // run + k0 is 16-byte aligned: paired loads
+      const double2* r2 = reinterpret_cast<const double2*>(run + k0);
 #pragma unroll
-    for (int q = 0; q < kDB; q += 4) {
-      if (q < nb) v0 = fma(Dblk[q * kDB + lane], run[k0 + q], v0);
-      if (q + 1 < nb) v1 = fma(Dblk[(q + 1) * kDB + lane], run[k0 + q + 1], v1);
-      if (q + 2 < nb) v2 = fma(Dblk[(q + 2) * kDB + lane], run[k0 + q + 2], v2);
-      if (q + 3 < nb) v3 = fma(Dblk[(q + 3) * kDB + lane], run[k0 + q + 3], v3);
+      for (int q = 0; q < kDB; q += 4) {
+        const double2 ra = r2[q / 2], rb = r2[q / 2 + 1];
+        v0 = fma(Dblk[q * kDB + lane], ra.x, v0);
+        v1 = fma(Dblk[(q + 1) * kDB + lane], ra.y, v1);
+        v2 = fma(Dblk[(q + 2) * kDB + lane], rb.x, v2);
+        v3 = fma(Dblk[(q + 3) * kDB + lane], rb.y, v3);
+      }
+    } else {
+      for (int q = 0; q < nb; ++q) v0 = fma(Dblk[q * kDB + lane], run[k0 + q], v0);
     }
-    const double v = (v0 + v1) + (v2 + v3);
-    yw[lane] = v;
-    if (warp == 0 && lane < nb) res[k0 + lane] = v;
-    __syncwarp();
-    stage(t + 1, (t + 1) & 1);
-    for (int i = i0 + tid; i < i1; i += NT) {
-      const double* a = A + (size_t)k0 * m + i;
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-      if (nb == kDB) {
-        double tq[kDB];
+    return (v0 + v1) + (v2 + v3);
+  };
+  // run[i] -= A[i, k0 .. k0+nb) y for row i, tq preloaded when `have`
+  auto row = [&](int k0, int nb, int i, const double* y, double (&tq)[kDB], bool have,
+                 double* run) {
+    const double* a = A + (size_t)k0 * m + i;
+    double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+    if (nb == kDB) {
+      if (!have) {
 #pragma unroll
         for (int q = 0; q < kDB; ++q) tq[q] = a[(size_t)q * m];
-#pragma unroll
-        for (int q = 0; q < kDB; q += 4) {
-          s0 = fma(tq[q], yw[q], s0);
-          s1 = fma(tq[q + 1], yw[q + 1], s1);
-          s2 = fma(tq[q + 2], yw[q + 2], s2);
-          s3 = fma(tq[q + 3], yw[q + 3], s3);
-        }
-      } else {
-        for (int q = 0; q < nb; ++q) s0 = fma(a[(size_t)q * m], yw[q], s0);
       }
-      run[i] -= (s0 + s1) + (s2 + s3);
+      const double2* y2 = reinterpret_cast<const double2*>(y);
+#pragma unroll
+      for (int q = 0; q < kDB; q += 4) {
+        const double2 ya = y2[q / 2], yb = y2[q / 2 + 1];
+        s0 = fma(tq[q], ya.x, s0);
+        s1 = fma(tq[q + 1], ya.y, s1);
+        s2 = fma(tq[q + 2], yb.x, s2);
+        s3 = fma(tq[q + 3], yb.y, s3);
+      }
+    } else {
+      for (int q = 0; q < nb; ++q) s0 = fma(a[(size_t)q * m], y[q], s0);
+    }
+    run[i] -= (s0 + s1) + (s2 + s3);
+  };
+  auto step = [&](int t, int k0, int nb, double* run, double* res, int i0, int i1) {
+    double tq[kDB];
+    if constexpr (NT >= 512) {
+      // warp 0 forms y and shares it through shared memory (one more barrier,
+      // against 16 warps each reading the 8 KB block); the first row's panel
+      // values are loaded meanwhile
+      const int ifirst = i0 + tid;
+      const bool pre = ifirst < i1 && nb == kDB;
+      if (pre) {
+        const double* a = A + (size_t)k0 * m + ifirst;
+#pragma unroll
+        for (int q = 0; q < kDB; ++q) tq[q] = a[(size_t)q * m];
+      }
+      if (warp == 0) {
+        const double v = diag(t, k0, nb, run);
+        ys[lane] = v;
+        if (lane < nb) res[k0 + lane] = v;
+      }
+      stage(t + 1, (t + 1) & 1);
+      __syncthreads();
+      for (int i = ifirst; i < i1; i += NT) row(k0, nb, i, ys, tq, pre && i == ifirst, run);
+    } else {
+      // every warp forms y itself (no barrier before the rows)
+      double* yw = ys + 32 * warp;
+      const double v = diag(t, k0, nb, run);
+      yw[lane] = v;
+      if (warp == 0 && lane < nb) res[k0 + lane] = v;
+      __syncwarp();
+      stage(t + 1, (t + 1) & 1);
+      for (int i = i0 + tid; i < i1; i += NT) row(k0, nb, i, yw, tq, false, run);
     }
     asm volatile("cp.async.wait_group 0;\n" ::);
     __syncthreads();
