@@ -333,18 +333,26 @@ def gpu_arm(args):
                                    theta=w["theta"], kappa=kap, eps0=w["eps0"], eps1=w["eps1"],
                                    tol=w["tol"])
 
+    # the step's inputs in page-locked host memory (as a caller streaming
+    # molecules would hold them); the tensors keep the buffers alive
+    pinned_t = {k: torch.from_numpy(np.ascontiguousarray(inp[k], dtype=dt)).pin_memory()
+                for k, dt in (("sptpos", np.float64), ("sptnrm", np.float64),
+                              ("nvert", np.int32), ("chrpos", np.float64),
+                              ("atmchr", np.float64))}
+    pin = {k: t.numpy() for k, t in pinned_t.items()}
+
     def e2e_once():
         nonlocal h2d, d2h
         s = e2e_solver
-        xyz, tq, ar, b = s.form_matrix(inp["sptpos"], inp["sptnrm"], inp["nvert"],
-                                       inp["chrpos"], inp["atmchr"])
+        xyz, tq, ar, b = s.form_matrix(pin["sptpos"], pin["sptnrm"], pin["nvert"],
+                                       pin["chrpos"], pin["atmchr"])
         s.build_tree()
         _, _, _, bt = s.permute(bvct=b)
         r = s.dgmres(bt)
-        se, ce = s.energy(inp["chrpos"], inp["atmchr"], r["x"])
-        h2d = (inp["sptpos"].nbytes + inp["sptnrm"].nbytes + inp["nvert"].nbytes
-               + inp["chrpos"].nbytes + inp["atmchr"].nbytes + 2 * bt.nbytes
-               + inp["chrpos"].nbytes + inp["atmchr"].nbytes + r["x"].nbytes)
+        se, ce = s.energy(pin["chrpos"], pin["atmchr"], r["x"])
+        h2d = (pin["sptpos"].nbytes + pin["sptnrm"].nbytes + pin["nvert"].nbytes
+               + pin["chrpos"].nbytes + pin["atmchr"].nbytes + 2 * bt.nbytes
+               + pin["chrpos"].nbytes + pin["atmchr"].nbytes + r["x"].nbytes)
         d2h = (xyz.nbytes + tq.nbytes + ar.nbytes + b.nbytes + 4 * nface + r["x"].nbytes + 16)
         return se
 
