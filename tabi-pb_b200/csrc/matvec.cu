@@ -122,10 +122,10 @@ __global__ void mom_final_kernel(const int2* __restrict__ mslot_chunks,
 // T = double: the reference's arithmetic.  T = float (mixed precision): the
 // target-to-centre offset is formed in FP64 and rounded once, the Taylor
 // recurrences and the contraction run in FP32, the result is widened to FP64
-// for the per-target sum.  Order 3 in FP64 is capped at 128 registers (8
-// blocks per SM instead of 6, for a few bytes of spill).
+// for the per-target sum.  Order 3 is capped at 128 registers (8 blocks per
+// SM instead of 6 in FP64, for a few bytes of spill).
 template <int P, typename T>
-__global__ void __launch_bounds__(64, (P == 3 && sizeof(T) == 8) ? 8 : 1) far_kernel(const WorkItem* __restrict__ work,
+__global__ void __launch_bounds__(64, P == 3 ? 8 : 1) far_kernel(const WorkItem* __restrict__ work,
                                                  const int2* __restrict__ ent,
                                                  const T* __restrict__ mw,
                                                  const double* __restrict__ nd_mid,
