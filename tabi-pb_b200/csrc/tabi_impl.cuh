@@ -45,10 +45,15 @@ template <typename T>
 struct DBuf {
   T* p = nullptr;
   size_t n = 0;
+  // Grows only.  A buffer that has to grow again gets 1.5x the request: every
+  // cudaFree synchronises the whole device, which stalls the other handles'
+  // work (batch workers share the GPU), so regrowth should be rare.
   void alloc(size_t count) {
     if (count <= n && p) return;
+    const bool regrow = p != nullptr;
     release();
     if (count == 0) return;
+    if (regrow) count += count / 2;
     TABI_CUDA(cudaMalloc(&p, count * sizeof(T)));
     n = count;
   }
