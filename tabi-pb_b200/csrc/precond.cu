@@ -1398,15 +1398,16 @@ void build_precond(Handle& H, cudaStream_t s) {
             TABI_CUDA(cudaEventRecord(H.ev_fork, s));
             TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
           }
-          // the register-resident panel up to 512 x kRegMaxRows rows left, the
-          // shared-memory one above
+          // the register-resident panel up to 512 x kRegMaxRows rows left (the
+          // fewest warps that hold the rows, one row per thread below 257
+          // rows), the shared-memory one above
           auto panel = [&](int cnt, const int* list, int mr, cudaStream_t st) {
             TABI_K(K_LU, st);
             if (mr <= 256)
               lu_panel_reg_kernel<256, 1><<<cnt, 256, 0, st>>>(
                   list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
             else if (mr <= 512)
-              lu_panel_reg_kernel<512, 1><<<cnt, 512, 0, st>>>(
+              lu_panel_reg_kernel<256, 2><<<cnt, 256, 0, st>>>(
                   list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
             else if (mr <= 512 * kRegMaxRows)
               lu_panel_reg_kernel<512, kRegMaxRows><<<cnt, 512, 0, st>>>(
