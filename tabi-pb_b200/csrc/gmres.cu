@@ -397,7 +397,7 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
 // the FP64 operator and measures it the way DGMRES does for ITOL = 2,
 // |M^-1 r| / |M^-1 b|; while that is above tol, GMRES (FP64 vectors, Arnoldi
 // and Givens, FP32 operator) solves A d = r to the relative tolerance
-// tol * |M^-1 b| / |M^-1 r| and x += d.  The FP64 residual is the judge: the
+// tol * |M^-1 b| / |M^-1 r| and x += d.  The FP64 residual decides: the
 // solve stops only when it is below tol.  iter counts the inner iterations,
 // err is the final FP64 measure, err_hist the inner estimates rescaled to
 // |M^-1 b| (at most (nrmax+1)*maxl of them, the same cap as the FP64 path,

@@ -3,8 +3,8 @@
 // potential and normal derivative x0 = [phi; dphi/dn] of a solve from the
 // panel geometry and the right-hand side (main.f90:592-606).  It has no
 // counterpart in the reference, which always starts GMRES from zero
-// (main.f90:133); GMRES on the true residual stays the judge, so a prediction
-// only changes the iteration count.
+// (main.f90:133); GMRES on the true residual still decides convergence, so a
+// prediction only changes the iteration count.
 //
 // Network, for N panels (centroid r, unit normal n, area A, b = [b1; b2], and
 // z = M^-1 b, the leaf-block preconditioner's solution -- exact within each

@@ -8,7 +8,7 @@ benchmark's atom density and 10 vertices/A^2 surfaces) with atom counts
 log-uniform in [--min-atoms, --max-atoms], seeds 10000 + k; held-out
 molecules: --test-atoms atoms, seeds 90000 + k.  Each is solved from zero to
 --tol (mixed precision); the network is trained on those solutions and then
-judged by the GMRES iterations and solve time to --tol from its prediction
+evaluated by the GMRES iterations and solve time to --tol from its prediction
 against from zero, on the held-out set.  Surfaces are generated by a pool of
 host processes (started before the GPU is touched).
 """
