@@ -266,7 +266,7 @@ constexpr int kUT = 256;           // strip / gemm kernel threads
 constexpr int kUC = 128;           // strip width
 constexpr int kGT = 64;            // gemm tile
 constexpr int kOB = 256;           // outer block: columns right of it are updated once per block
-constexpr int kPanelSmall = 320;   // rows left: panels up to this run in their own launch
+constexpr int kLuSmallBlock = 512; // blocks up to this order factor on the side stream
 
 // Factor columns [c0l, c0l + nb) of the panel held in P (local column c of
 // the half is P + c * mr, local row r = global row k0 + r) starting at local
@@ -1284,173 +1284,180 @@ void build_precond(Handle& H, cudaStream_t s) {
       if (m <= kPanelMaxM) mmax = std::max(mmax, m);
       else any_big = true;
     }
-    const int nsteps = (mmax + kBP - 1) / kBP;
-    std::vector<int> order(nl);
-    for (int l = 0; l < nl; ++l) order[l] = l;
-    std::sort(order.begin(), order.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
-    // Two-level right-looking LU (LAPACK DGETRF order).  Outer blocks of kOB
-    // columns; inside one, 32-column panel steps update only the block's own
-    // columns (and swap the columns left of the panel).  After the block its
-    // kOB row interchanges are applied at once to the columns right of it,
-    // U12 follows by four 32-row TRSM + small GEMM steps, and the trailing
-    // matrix gets one kOB-deep update.
-    struct Launch {
-      int kind;  // 0 panel, 1 strip, 2 gemm, 3 swap map, 4 row swap
-      int k0, kdepth, off, cnt;
-    };
-    std::vector<Launch> plan;
-    std::vector<int> pitems, mleaves;
-    std::vector<int4> sitems, gitems, ritems;
-    auto emit = [&](int kind, int k0, int kdepth, size_t before, size_t after) {
-      if (after > before) plan.push_back({kind, k0, kdepth, (int)before, (int)(after - before)});
-    };
-    const auto pack = [](int re, int ce) { return (re << 16) | ce; };
-    for (int K0 = 0; K0 < mmax; K0 += kOB) {
-      for (int k0 = K0; k0 < std::min(mmax, K0 + kOB); k0 += kBP) {
-        size_t p0 = pitems.size(), s0 = sitems.size(), g0 = gitems.size();
-        for (int l : order) {
-          const int m = 2 * rng[l].y;
-          if (m > kPanelMaxM || m <= k0) continue;
-          pitems.push_back(l);
-          const int nb = std::min(kBP, m - k0), ce = std::min(m, K0 + kOB);
-          // left of the panel inside the outer block (the columns left of
-          // the block get the block's swaps at its end)
-          for (int c0 = K0; c0 < k0; c0 += kUC)
-            sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, k0), 0));
-          for (int c0 = k0 + nb; c0 < ce; c0 += kUC)
-            sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, ce), 1));
-          for (int r0 = k0 + nb; r0 < m; r0 += kGT)
-            for (int c0 = k0 + nb; c0 < ce; c0 += kGT)
-              gitems.push_back(make_int4(l, r0, c0, pack(m, ce)));
-        }
-        emit(0, k0, 0, p0, pitems.size());
-        emit(1, k0, 0, s0, sitems.size());
-        emit(2, k0, kBP, g0, gitems.size());
-      }
-      // the block's row interchanges on the columns left of it and right of it
-      const int Kend = K0 + kOB;
-      size_t m0 = mleaves.size(), r0i = ritems.size();
-      for (int l : order) {
-        const int m = 2 * rng[l].y;
-        if (m > kPanelMaxM || m <= K0 || (K0 == 0 && m <= Kend)) continue;
-        const int slot = (int)(mleaves.size() - m0);
-        mleaves.push_back(l);
-        for (int c0 = 0; c0 < K0; c0 += kUC)
-          ritems.push_back(make_int4(slot, c0, std::min(c0 + kUC, K0), l));
-        for (int c0 = Kend; c0 < m; c0 += kUC)
-          ritems.push_back(make_int4(slot, c0, std::min(c0 + kUC, m), l));
-      }
-      emit(3, K0, 0, m0, mleaves.size());
-      emit(4, K0, 0, r0i, ritems.size());
-      for (int kb = K0; kb < Kend; kb += kBP) {
-        size_t s0 = sitems.size(), g0 = gitems.size();
-        for (int l : order) {
-          const int m = 2 * rng[l].y;
-          if (m > kPanelMaxM || m <= Kend) continue;
-          for (int c0 = Kend; c0 < m; c0 += kUC)
-            sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, m), 3));
-          for (int rr = kb + kBP; rr < Kend; rr += kGT)
-            for (int c0 = Kend; c0 < m; c0 += kGT)
-              gitems.push_back(make_int4(l, rr, c0, pack(Kend, m)));
-        }
-        emit(1, kb, 0, s0, sitems.size());
-        emit(2, kb, kBP, g0, gitems.size());
-      }
-      size_t g0 = gitems.size();
-      for (int l : order) {
-        const int m = 2 * rng[l].y;
-        if (m > kPanelMaxM || m <= Kend) continue;
-        for (int rr = Kend; rr < m; rr += kGT)
-          for (int c0 = Kend; c0 < m; c0 += kGT) gitems.push_back(make_int4(l, rr, c0, 0));
-      }
-      emit(2, K0, kOB, g0, gitems.size());
-    }
-    auto up = [&](auto& buf, const auto& v) {
-      buf.alloc(std::max<size_t>(v.size(), 1));
-      if (!v.empty())
-        TABI_CUDA(cudaMemcpyAsync(buf.p, v.data(), sizeof(v[0]) * v.size(),
-                                  cudaMemcpyHostToDevice, s));
-    };
-    up(H.pc_list, pitems);
-    up(H.pc_items, sitems);
-    up(H.pc_gitems, gitems);
-    up(H.pc_mleaves, mleaves);
-    up(H.pc_ritems, ritems);
-    size_t maxm = 1;
-    for (const Launch& L : plan)
-      if (L.kind == 3) maxm = std::max<size_t>(maxm, (size_t)L.cnt);
-    H.pc_map.alloc(maxm * (4 * kOB + 1));
-    if (nsteps > 0) {
+    if (mmax > 0) {
       size_t smem = sizeof(double) * (size_t)mmax * kSP;
       raise_smem_limit((const void*)lu_panel_kernel, std::max<size_t>(smem, 48 * 1024));
     }
     raise_smem_limit((const void*)lu_gemm_kernel, kGemmSmem);
-    for (const Launch& L : plan) {
-      switch (L.kind) {
-        case 0: {
-          // items are largest first; shared memory is sized by a launch's
-          // largest block, so blocks with at most kPanelSmall rows left run in
-          // a second launch (several CTAs per SM) on the side stream
-          int nbig = 0;
-          while (nbig < L.cnt && 2 * rng[pitems[L.off + nbig]].y - L.k0 > kPanelSmall) ++nbig;
-          const bool fork = nbig > 0 && nbig < L.cnt && H.side != nullptr;
-          if (fork) {
-            TABI_CUDA(cudaEventRecord(H.ev_fork, s));
-            TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
+    // Two leaf groups with plans of their own: blocks of order above
+    // kLuSmallBlock on the handle's stream, the others on its side stream, so
+    // the many short factorisations of small leaves run beside the long
+    // panel chain of the large ones instead of inside its launches; one fork
+    // after the assembly, one join at the end.
+    std::vector<int> grp[2];
+    for (int l = 0; l < nl; ++l) {
+      const int m = 2 * rng[l].y;
+      if (m <= kPanelMaxM) grp[m > kLuSmallBlock ? 0 : 1].push_back(l);
+    }
+    for (auto& g : grp)
+      std::sort(g.begin(), g.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
+    const bool split = H.side != nullptr && !grp[0].empty() && !grp[1].empty();
+    if (split) {
+      TABI_CUDA(cudaEventRecord(H.ev_fork, s));
+      TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
+    }
+    // Two-level right-looking LU (LAPACK DGETRF order) of one group.  Outer
+    // blocks of kOB columns; inside one, 32-column panel steps update only
+    // the block's own columns (and swap the columns left of the panel).  After
+    // the block its kOB row interchanges are applied at once to the columns
+    // right of it, U12 follows by 32-row TRSM + small GEMM steps, and the
+    // trailing matrix gets one kOB-deep update.
+    auto run_group = [&](const std::vector<int>& order, Handle::LuPlan& B, cudaStream_t st) {
+      int gmax = 0;
+      for (int l : order) gmax = std::max(gmax, 2 * rng[l].y);
+      struct Launch {
+        int kind;  // 0 panel, 1 strip, 2 gemm, 3 swap map, 4 row swap
+        int k0, kdepth, off, cnt;
+      };
+      std::vector<Launch> plan;
+      std::vector<int> pitems, mleaves;
+      std::vector<int4> sitems, gitems, ritems;
+      auto emit = [&](int kind, int k0, int kdepth, size_t before, size_t after) {
+        if (after > before) plan.push_back({kind, k0, kdepth, (int)before, (int)(after - before)});
+      };
+      const auto pack = [](int re, int ce) { return (re << 16) | ce; };
+      for (int K0 = 0; K0 < gmax; K0 += kOB) {
+        for (int k0 = K0; k0 < std::min(gmax, K0 + kOB); k0 += kBP) {
+          size_t p0 = pitems.size(), s0 = sitems.size(), g0 = gitems.size();
+          for (int l : order) {
+            const int m = 2 * rng[l].y;
+            if (m <= k0) continue;
+            pitems.push_back(l);
+            const int nb = std::min(kBP, m - k0), ce = std::min(m, K0 + kOB);
+            // left of the panel inside the outer block (the columns left of
+            // the block get the block's swaps at its end)
+            for (int c0 = K0; c0 < k0; c0 += kUC)
+              sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, k0), 0));
+            for (int c0 = k0 + nb; c0 < ce; c0 += kUC)
+              sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, ce), 1));
+            for (int r0 = k0 + nb; r0 < m; r0 += kGT)
+              for (int c0 = k0 + nb; c0 < ce; c0 += kGT)
+                gitems.push_back(make_int4(l, r0, c0, pack(m, ce)));
           }
-          // the register-resident panel up to 512 x kRegMaxRows rows left (the
-          // fewest warps that hold the rows, one row per thread below 257
-          // rows), the shared-memory one above
-          auto panel = [&](int cnt, const int* list, int mr, cudaStream_t st) {
+          emit(0, k0, 0, p0, pitems.size());
+          emit(1, k0, 0, s0, sitems.size());
+          emit(2, k0, kBP, g0, gitems.size());
+        }
+        // the block's row interchanges on the columns left of it and right of it
+        const int Kend = K0 + kOB;
+        size_t m0 = mleaves.size(), r0i = ritems.size();
+        for (int l : order) {
+          const int m = 2 * rng[l].y;
+          if (m <= K0 || (K0 == 0 && m <= Kend)) continue;
+          const int slot = (int)(mleaves.size() - m0);
+          mleaves.push_back(l);
+          for (int c0 = 0; c0 < K0; c0 += kUC)
+            ritems.push_back(make_int4(slot, c0, std::min(c0 + kUC, K0), l));
+          for (int c0 = Kend; c0 < m; c0 += kUC)
+            ritems.push_back(make_int4(slot, c0, std::min(c0 + kUC, m), l));
+        }
+        emit(3, K0, 0, m0, mleaves.size());
+        emit(4, K0, 0, r0i, ritems.size());
+        for (int kb = K0; kb < Kend; kb += kBP) {
+          size_t s0 = sitems.size(), g0 = gitems.size();
+          for (int l : order) {
+            const int m = 2 * rng[l].y;
+            if (m <= Kend) continue;
+            for (int c0 = Kend; c0 < m; c0 += kUC)
+              sitems.push_back(make_int4(l, c0, std::min(c0 + kUC, m), 3));
+            for (int rr = kb + kBP; rr < Kend; rr += kGT)
+              for (int c0 = Kend; c0 < m; c0 += kGT)
+                gitems.push_back(make_int4(l, rr, c0, pack(Kend, m)));
+          }
+          emit(1, kb, 0, s0, sitems.size());
+          emit(2, kb, kBP, g0, gitems.size());
+        }
+        size_t g0 = gitems.size();
+        for (int l : order) {
+          const int m = 2 * rng[l].y;
+          if (m <= Kend) continue;
+          for (int rr = Kend; rr < m; rr += kGT)
+            for (int c0 = Kend; c0 < m; c0 += kGT) gitems.push_back(make_int4(l, rr, c0, 0));
+        }
+        emit(2, K0, kOB, g0, gitems.size());
+      }
+      auto up = [&](auto& buf, const auto& v) {
+        buf.alloc(std::max<size_t>(v.size(), 1));
+        if (!v.empty())
+          TABI_CUDA(cudaMemcpyAsync(buf.p, v.data(), sizeof(v[0]) * v.size(),
+                                    cudaMemcpyHostToDevice, st));
+      };
+      up(B.list, pitems);
+      up(B.items, sitems);
+      up(B.gitems, gitems);
+      up(B.mleaves, mleaves);
+      up(B.ritems, ritems);
+      size_t maxm = 1;
+      for (const Launch& L : plan)
+        if (L.kind == 3) maxm = std::max<size_t>(maxm, (size_t)L.cnt);
+      B.map.alloc(maxm * (4 * kOB + 1));
+      for (const Launch& L : plan) {
+        switch (L.kind) {
+          case 0: {
+            // the register-resident panel up to 512 x kRegMaxRows rows left
+            // (the fewest warps that hold the rows, one row per thread below
+            // 257 rows), the shared-memory one above; a launch is sized by its
+            // first (largest) block
+            const int mr = 2 * rng[pitems[L.off]].y - L.k0;
+            const int* list = B.list.p + L.off;
             TABI_K(K_LU, st);
             if (mr <= 256)
-              lu_panel_reg_kernel<256, 1><<<cnt, 256, 0, st>>>(
+              lu_panel_reg_kernel<256, 1><<<L.cnt, 256, 0, st>>>(
                   list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
             else if (mr <= 512)
-              lu_panel_reg_kernel<256, 2><<<cnt, 256, 0, st>>>(
+              lu_panel_reg_kernel<256, 2><<<L.cnt, 256, 0, st>>>(
                   list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
             else if (mr <= 512 * kRegMaxRows)
-              lu_panel_reg_kernel<512, kRegMaxRows><<<cnt, 512, 0, st>>>(
+              lu_panel_reg_kernel<512, kRegMaxRows><<<L.cnt, 512, 0, st>>>(
                   list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
             else
-              lu_panel_kernel<<<cnt, kPT, sizeof(double) * (size_t)mr * kSP, st>>>(
+              lu_panel_kernel<<<L.cnt, kPT, sizeof(double) * (size_t)mr * kSP, st>>>(
                   list, L.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p);
-          };
-          if (nbig > 0) panel(nbig, H.pc_list.p + L.off, 2 * rng[pitems[L.off]].y - L.k0, s);
-          if (nbig < L.cnt)
-            panel(L.cnt - nbig, H.pc_list.p + L.off + nbig,
-                  2 * rng[pitems[L.off + nbig]].y - L.k0, fork ? H.side : s);
-          if (fork) {
-            TABI_CUDA(cudaEventRecord(H.ev_join, H.side));
-            TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
+            break;
           }
-          break;
-        }
-        case 1: {
-          TABI_K(K_LU_STRIP, s);
-          lu_strip_kernel<<<L.cnt, kUT, 0, s>>>(H.pc_items.p + L.off, L.k0, T.d_leaf_rng.p,
-                                                T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
-          break;
-        }
-        case 2: {
-          TABI_K(K_LU_UPDATE, s);
-          lu_gemm_kernel<<<L.cnt, kUT, kGemmSmem, s>>>(H.pc_gitems.p + L.off, L.k0, L.kdepth,
-                                                       T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p);
-          break;
-        }
-        case 3: {
-          TABI_K(K_LU_SWAP, s);
-          lu_swapmap_kernel<<<L.cnt, 256, 0, s>>>(H.pc_mleaves.p + L.off, L.k0, T.d_leaf_rng.p,
-                                                  T.d_piv.p, H.pc_map.p);
-          break;
-        }
-        case 4: {
-          TABI_K(K_LU_SWAP, s);
-          lu_rowswap_kernel<<<L.cnt, kUT, 0, s>>>(H.pc_ritems.p + L.off, T.d_leaf_rng.p,
-                                                  T.d_blk_off.p, H.pc_map.p, T.d_lu.p);
-          break;
+          case 1: {
+            TABI_K(K_LU_STRIP, st);
+            lu_strip_kernel<<<L.cnt, kUT, 0, st>>>(B.items.p + L.off, L.k0, T.d_leaf_rng.p,
+                                                   T.d_blk_off.p, T.d_lu.p, T.d_piv.p);
+            break;
+          }
+          case 2: {
+            TABI_K(K_LU_UPDATE, st);
+            lu_gemm_kernel<<<L.cnt, kUT, kGemmSmem, st>>>(B.gitems.p + L.off, L.k0, L.kdepth,
+                                                          T.d_leaf_rng.p, T.d_blk_off.p,
+                                                          T.d_lu.p);
+            break;
+          }
+          case 3: {
+            TABI_K(K_LU_SWAP, st);
+            lu_swapmap_kernel<<<L.cnt, 256, 0, st>>>(B.mleaves.p + L.off, L.k0,
+                                                     T.d_leaf_rng.p, T.d_piv.p, B.map.p);
+            break;
+          }
+          case 4: {
+            TABI_K(K_LU_SWAP, st);
+            lu_rowswap_kernel<<<L.cnt, kUT, 0, st>>>(B.ritems.p + L.off, T.d_leaf_rng.p,
+                                                     T.d_blk_off.p, B.map.p, T.d_lu.p);
+            break;
+          }
         }
       }
+    };
+    if (!grp[0].empty()) run_group(grp[0], H.pc_plan[0], s);
+    if (!grp[1].empty()) run_group(grp[1], H.pc_plan[1], split ? H.side : s);
+    if (split) {
+      TABI_CUDA(cudaEventRecord(H.ev_join, H.side));
+      TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
     }
     if (any_big) {
       TABI_K(K_LU, s);

@@ -297,8 +297,14 @@ struct Handle {
   DBuf<int> ls_tgt, ls_far, ls_near;
   DBuf<int64_t> ls_bsum, ls_foff, ls_noff;
   DBuf<int2> pc_tiles;
-  DBuf<int> pc_info, pc_list, pc_mleaves, pc_map;
-  DBuf<int4> pc_items, pc_gitems, pc_ritems;
+  DBuf<int> pc_info;
+  // one LU plan per leaf group (large blocks on the handle's stream, small
+  // ones on its side stream): panel leaves, strip / gemm / row-swap items,
+  // swap-map leaves and maps
+  struct LuPlan {
+    DBuf<int> list, mleaves, map;
+    DBuf<int4> items, gitems, ritems;
+  } pc_plan[2];
   DBuf<int2> pc_dblocks;
   // staging of the host-array entry points and of tabi_run_dev
   DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;
