@@ -333,22 +333,31 @@ def gpu_arm(args):
                                    theta=w["theta"], kappa=kap, eps0=w["eps0"], eps1=w["eps1"],
                                    tol=w["tol"])
 
-    # the step's inputs in page-locked host memory (as a caller streaming
-    # molecules would hold them); the tensors keep the buffers alive
+    # the step's inputs and outputs in page-locked host memory (as a caller
+    # streaming molecules would hold them); the tensors keep the buffers alive
     pinned_t = {k: torch.from_numpy(np.ascontiguousarray(inp[k], dtype=dt)).pin_memory()
                 for k, dt in (("sptpos", np.float64), ("sptnrm", np.float64),
                               ("nvert", np.int32), ("chrpos", np.float64),
                               ("atmchr", np.float64))}
     pin = {k: t.numpy() for k, t in pinned_t.items()}
+    # and the arrays the step reads back
+    nf = len(inp["nvert"])
+    for k, shape in (("xyz", (nf, 3)), ("tq", (nf, 3)), ("ar", (nf,)), ("b", (2 * nf,)),
+                     ("bt", (2 * nf,)), ("x", (2 * nf,))):
+        pinned_t[k] = torch.empty(shape, dtype=torch.float64).pin_memory()
+        pin[k] = pinned_t[k].numpy()
 
     def e2e_once():
         nonlocal h2d, d2h
         s = e2e_solver
         xyz, tq, ar, b = s.form_matrix(pin["sptpos"], pin["sptnrm"], pin["nvert"],
-                                       pin["chrpos"], pin["atmchr"])
+                                       pin["chrpos"], pin["atmchr"],
+                                       out=(pin["xyz"], pin["tq"], pin["ar"], pin["b"]))
         s.build_tree()
         _, _, _, bt = s.permute(bvct=b)
-        r = s.dgmres(bt)
+        pin["bt"][:] = bt
+        bt = pin["bt"]
+        r = s.dgmres(bt, out=pin["x"])
         se, ce = s.energy(pin["chrpos"], pin["atmchr"], r["x"])
         h2d = (pin["sptpos"].nbytes + pin["sptnrm"].nbytes + pin["nvert"].nbytes
                + pin["chrpos"].nbytes + pin["atmchr"].nbytes + 2 * bt.nbytes

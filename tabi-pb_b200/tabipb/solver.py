@@ -76,17 +76,22 @@ class TabiSolver:
         return self.params.eps1 / self.params.eps0
 
     # ---- main.f90:546-610
-    def form_matrix(self, sptpos, sptnrm, nvert, chrpos, atmchr):
+    def form_matrix(self, sptpos, sptnrm, nvert, chrpos, atmchr, out=None):
+        """out: optional (tr_xyz (n,3), tr_q (n,3), tr_area (n), bvct (2n))
+        float64 C-contiguous arrays to write into (e.g. page-locked ones)."""
         sp = f64(sptpos, (-1, 3))
         sn = f64(sptnrm, (-1, 3))
         nv = i32(nvert).reshape(-1, 3)
         cp = f64(chrpos, (-1, 3))
         q = f64(atmchr).ravel()
         n = nv.shape[0]
-        xyz = np.zeros((n, 3))
-        tq = np.zeros((n, 3))
-        ar = np.zeros(n)
-        b = np.zeros(2 * n)
+        if out is None:
+            xyz, tq, ar, b = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros(n), np.zeros(2 * n)
+        else:
+            xyz, tq, ar, b = out
+            for a, shape in ((xyz, (n, 3)), (tq, (n, 3)), (ar, (n,)), (b, (2 * n,))):
+                if a.shape != shape or a.dtype != np.float64 or not a.flags.c_contiguous:
+                    raise ValueError(f"out array of shape {shape}, float64, C order expected")
         check(self.h, self.L.tabi_form_matrix(self.h, sp.shape[0], dptr(sp), dptr(sn), n,
                                               iptr(nv), cp.shape[0], dptr(cp), dptr(q),
                                               dptr(xyz), dptr(tq), dptr(ar), dptr(b)))
@@ -154,9 +159,16 @@ class TabiSolver:
         check(self.h, self.L.tabi_msolve(self.h, r.size, dptr(r), dptr(z)))
         return z
 
-    def dgmres(self, b, x0=None):
+    def dgmres(self, b, x0=None, out=None):
+        """out: optional float64 array of 2n for the solution (e.g. page-locked)."""
         b = f64(b).ravel()
-        x = np.zeros_like(b) if x0 is None else f64(x0).ravel().copy()
+        if out is None:
+            x = np.zeros_like(b) if x0 is None else f64(x0).ravel().copy()
+        else:
+            if out.shape != b.shape or out.dtype != np.float64 or not out.flags.c_contiguous:
+                raise ValueError("out must be a float64 C-order array like b")
+            x = out
+            x[:] = 0.0 if x0 is None else f64(x0).ravel()
         it, ierr, nh = C.c_int(), C.c_int(), C.c_int()
         err = C.c_double()
         hist = np.zeros((self.params.nrmax + 1) * max(self.params.maxl, 1) + 2)

@@ -81,3 +81,28 @@ def test_bad_surfaces_and_vectors(gpu_lib):
     y_fresh, _ = _matvec_of(case, x)
     assert np.all(np.isfinite(y))
     assert np.array_equal(y, y_fresh)
+
+
+def test_caller_buffers(gpu_lib):
+    """form_matrix and dgmres write into caller-owned arrays (page-locked ones,
+    for instance) with results identical to the allocating calls; arrays of
+    the wrong shape are refused before the library is called."""
+    case = born_case(2)
+    with _solver() as s:
+        a = s.form_matrix(case["sptpos"], case["sptnrm"], case["nvert"], case["chrpos"],
+                          case["atmchr"])
+        n = s.nface
+        out = (np.empty((n, 3)), np.empty((n, 3)), np.empty(n), np.empty(2 * n))
+        b = s.form_matrix(case["sptpos"], case["sptnrm"], case["nvert"], case["chrpos"],
+                          case["atmchr"], out=out)
+        assert all(np.array_equal(u, v) for u, v in zip(a, b))
+        assert all(u is v for u, v in zip(b, out))
+        with pytest.raises(ValueError):
+            s.form_matrix(case["sptpos"], case["sptnrm"], case["nvert"], case["chrpos"],
+                          case["atmchr"], out=(out[0], out[1], out[2], np.empty(n)))
+        s.build_tree()
+        _, _, _, bt = s.permute(bvct=b[3])
+        r1 = s.dgmres(bt)
+        x = np.full(2 * n, 7.0)
+        r2 = s.dgmres(bt, out=x)
+        assert r2["x"] is x and np.array_equal(r1["x"], x) and r1["iter"] == r2["iter"]
