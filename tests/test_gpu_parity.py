@@ -51,6 +51,10 @@ CASES = {
     "mol60_L200": (lambda: molecule_case(60, 6.0, 2.0, seed=1), dict(maxparnode=200)),
     "mol60_p5_L150": (lambda: molecule_case(60, 6.0, 2.0, seed=2), dict(maxparnode=150, order=5,
                                                                          theta=0.7)),
+    # the large configuration's order and MAC, and the highest generated order
+    "mol60_p6_L100": (lambda: molecule_case(60, 6.0, 2.0, seed=4), dict(maxparnode=100, order=6,
+                                                                         theta=0.7)),
+    "born_l3_p8_L100": (lambda: born_case(3), dict(maxparnode=100, order=8, theta=0.6)),
 }
 
 
