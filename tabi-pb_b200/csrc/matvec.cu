@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(64, P == 3 ? 8 : 1) far_kernel(const WorkItem*
 
 // ---- near field
 constexpr int kNearThreads = 128;
-constexpr int kNearTile = 256;
+constexpr int kNearTile = 512;
 
 __global__ void __launch_bounds__(kNearThreads) near_kernel(
     const WorkItem* __restrict__ work, const int2* __restrict__ ent,
