@@ -252,7 +252,7 @@ __global__ void leaf_rel_kernel(const int* __restrict__ leaves, const int* __res
   }
 }
 
-constexpr int kNearTileF = 256;
+constexpr int kNearTileF = 512;
 
 __global__ void __launch_bounds__(kNearThreads) near_kernel_f32(
     const WorkItem* __restrict__ work, const int2* __restrict__ ent,
