@@ -269,7 +269,9 @@ void energy_dev(Handle& H, int nchr, const double* /*chrpos*/, const double* /*a
                 const double* x, double* soleng, double* couleng, cudaStream_t s) {
   const int n = H.n;
   int gx = ceil_div(nchr, kEA);
-  int gy = std::max(1, std::min(64, 296 * 2 / std::max(gx, 1)));
+  // face chunks per atom block: about six waves of the 2 x 148 resident
+  // blocks, so the last partial wave costs little
+  int gy = std::max(1, std::min(64, 296 * 6 / std::max(gx, 1)));
   H.d_ptl.alloc((size_t)gy * nchr + nchr);
   double eps = H.prm.eps1 / H.prm.eps0;
   { TABI_K(K_ENERGY, s); energy_kernel<<<dim3(gx, gy), kET, 0, s>>>(H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p, H.d_ny.p,
