@@ -17,8 +17,8 @@ Workload (one "step" = one complete TABI-PB solve of one molecule):
 ranks); `e2e` runs the same solve through the host-array C ABI
 (tabi_form_matrix ... tabi_energy) with the host<->device copies inside the
 timed region.  Multi-GPU runs are independent replicas (one molecule per
-rank, weak scaling).  `--impl reference` times the CPU restatement of the
-reference (oracle/, all host threads) on a bounded sample of the same solve.
+rank, weak scaling).  `--impl reference` times complete solves of the same
+molecule by the CPU restatement of the reference (oracle/, all host threads).
 """
 from __future__ import annotations
 
@@ -35,26 +35,14 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path[:0] = [os.path.join(ROOT, "tabi-pb_b200"), os.path.join(ROOT, "oracle")]
 
-WORKLOADS = {
-    # the benchmark configuration (see module docstring)
-    "globular": dict(natm=2000, radius=18.0, min_sep=2.0, density=10.0, probe=1.4, seed=0,
-                     order=3, theta=0.8, maxparnode=500, tol=1e-4, eps0=1.0, eps1=80.0,
-                     bulk=0.15, name="globular-2000-atoms-18A-10vA2-p3-mac0.8-leaf500-fp64"),
-    # a smaller molecule with the same settings, for profiler captures
-    "medium": dict(natm=600, radius=12.0, min_sep=2.0, density=10.0, probe=1.4, seed=0,
-                   order=3, theta=0.8, maxparnode=500, tol=1e-4, eps0=1.0, eps1=80.0,
-                   bulk=0.15, name="globular-600-atoms-12A-10vA2-p3-mac0.8-leaf500-fp64"),
-}
+from tabipb.workloads import WORKLOADS  # noqa: E402
+
 WORKLOAD = WORKLOADS["globular"]
 WORKLOAD_NAME = WORKLOAD["name"]
 METRIC = "solves/s (TABI-PB solve at <=1e-4 dG error; plain FP64)"
-# GMRES iterations of this workload, from the parity-checked GPU run (the
-# oracle reproduces the GPU's iteration count; used to scale the CPU sample)
-WORKLOAD_ITERS = None
 # trained warm-start network (tabipb.train_warmstart)
 WEIGHTS = os.path.join(ROOT, "tabi-pb_b200", "weights", "warmstart_h160_l3.npz")
 OPS_NEAR_PAIR = 64  # algorithmic ops per near-field pair (reference formulas)
-REF_BUDGET_S = 150.0  # wall-clock bound of the reference arm's timed steps
 
 
 def far_ops(p):
@@ -64,16 +52,9 @@ def far_ops(p):
 
 
 def make_inputs():
-    from tabipb import surface as S
+    from tabipb import workloads
 
-    w = WORKLOAD
-    xyz, q, r = S.synthetic_molecule(w["natm"], w["radius"], min_sep=w["min_sep"],
-                                     seed=w["seed"])
-    pos, nrm, fc, h = S.gaussian_surface(xyz, r, density=w["density"], probe=w["probe"])
-    fc, _ = S.face_filter(pos, fc)  # readin.f90:264-333
-    return dict(sptpos=np.ascontiguousarray(pos), sptnrm=np.ascontiguousarray(nrm),
-                nvert=np.ascontiguousarray(fc, dtype=np.int32),
-                chrpos=np.ascontiguousarray(xyz), atmchr=np.ascontiguousarray(q), grid=h)
+    return workloads.make_inputs(next(k for k, v in WORKLOADS.items() if v is WORKLOAD))
 
 
 class Clocks:
@@ -223,8 +204,10 @@ def gpu_arm(args):
                                                        "atmchr")}
     nspt, nface, natm = len(inp["sptpos"]), len(inp["nvert"]), len(inp["atmchr"])
     kap = tabipb.kappa(w["bulk"], w["eps1"])
+    flags = tabipb.FLAG_PIVOTED_LU if args.pivoted_lu else 0
     solver = tabipb.TabiSolver(order=w["order"], maxparnode=w["maxparnode"], theta=w["theta"],
-                               kappa=kap, eps0=w["eps0"], eps1=w["eps1"], tol=w["tol"])
+                               kappa=kap, eps0=w["eps0"], eps1=w["eps1"], tol=w["tol"],
+                               flags=flags)
     stream = torch.cuda.current_stream(dev)
     sp = stream.cuda_stream
 
@@ -326,7 +309,7 @@ def gpu_arm(args):
 
     # ---- end to end through the host-array C ABI: one handle (one molecule
     # at a time, buffers reused), host arrays in and out every step
-    e2e_steps = max(1, min(args.steps, 3))
+    e2e_steps = args.steps
     h2d = 0
     d2h = 0
     e2e_solver = tabipb.TabiSolver(order=w["order"], maxparnode=w["maxparnode"],
@@ -452,9 +435,7 @@ def gpu_arm(args):
 
 
 # ---------------------------------------------------------------- large mixed leg
-LARGE = dict(natm=20000, radius=40.0, min_sep=2.0, density=10.0, probe=1.4, seed=0, order=6,
-             theta=0.7, maxparnode=400, tol=1e-6, eps0=1.0, eps1=80.0, bulk=0.15,
-             name="large-20000-atoms-40A-10vA2-p6-mac0.7-leaf400-mixed-tol1e-6")
+LARGE = WORKLOADS["large"]
 
 
 def large_leg(args, dev):
@@ -467,12 +448,12 @@ def large_leg(args, dev):
     import torch
 
     import tabipb
-    from tabipb import surface as S
+    from tabipb import workloads
 
     w = LARGE
-    xyz, q, r = S.synthetic_molecule(w["natm"], w["radius"], min_sep=w["min_sep"], seed=w["seed"])
-    pos, nrm, fc, _ = S.gaussian_surface(xyz, r, density=w["density"], probe=w["probe"])
-    fc, _ = S.face_filter(pos, fc)
+    inp = workloads.make_inputs("large")
+    pos, nrm, fc, xyz, q = (inp["sptpos"], inp["sptnrm"], inp["nvert"], inp["chrpos"],
+                            inp["atmchr"])
     nspt, nface, natm = len(pos), len(fc), len(q)
     f = lambda a: torch.from_numpy(np.ascontiguousarray(a)).to(dev)
     d = dict(sptpos=f(pos), sptnrm=f(nrm), nvert=f(np.asarray(fc, np.int32)), chrpos=f(xyz),
@@ -615,47 +596,73 @@ def batched_leg(args, dev, rank):
 
 
 # ---------------------------------------------------------------- reference arm
+def oracle_solve(inp, nthreads):
+    """One complete solve by the CPU restatement of the reference (oracle/):
+    form_matrix -> tree -> DGMRES (the leaf blocks re-factored on every
+    preconditioner apply, as LEAFMATVECpara does) -> energy, on nthreads host
+    threads.  Returns (seconds per phase, result)."""
+    import oracle as O
+
+    w = WORKLOAD
+    kap = O.kappa(w["bulk"], w["eps1"])
+    eps = w["eps1"] / w["eps0"]
+    t0 = time.perf_counter()
+    xyz, tq, ar, b = O.form_matrix(inp["sptpos"], inp["sptnrm"], inp["nvert"], inp["chrpos"],
+                                   inp["atmchr"], w["eps0"], nthreads=nthreads)
+    t1 = time.perf_counter()
+    T = O.Tree(xyz, tq, ar, b, w["order"], w["maxparnode"], w["theta"])
+    t2 = time.perf_counter()
+    r = T.dgmres(kap, eps, T.bvct, iprcd=1, tol=w["tol"], nthreads=nthreads)
+    t3 = time.perf_counter()
+    se, ce = T.energy(inp["chrpos"], inp["atmchr"], kap, eps, w["eps0"], r["x"],
+                      nthreads=nthreads)
+    t4 = time.perf_counter()
+    t = dict(form=t1 - t0, tree=t2 - t1, dgmres=t3 - t2, energy=t4 - t3)
+    return t, dict(iter=r["iter"], ierr=r["ierr"], err=r["err"], soleng=se, couleng=ce,
+                   n_matvec=r["n_matvec"], n_msolve=r["n_msolve"])
+
+
 def reference_arm(args):
+    """The reference's CPU path on the host cores: every timed step is one
+    complete solve of the benchmark molecule by the oracle (the C restatement
+    of the reference; the Fortran cannot be built here) on all host threads.
+    The untimed warm-up steps run a bounded sample of the same code paths."""
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     if rank != 0:
         return
     nthreads = os.cpu_count() or 1
     inp = make_inputs()
-    iters = WORKLOAD_ITERS or args.iters
-    vals, parts, sample = [], None, ""
     for _ in range(args.warmup):
-        oracle_estimate(inp, iters, nthreads, target_sample=2048, leaf_sample=4, atom_sample=16,
+        oracle_estimate(inp, 6, nthreads, target_sample=2048, leaf_sample=4, atom_sample=16,
                         face_frac=0.05)
-    # the first timed step takes the full sample; later steps shrink theirs so
-    # that all steps together stay within about REF_BUDGET_S seconds
     t0 = time.perf_counter()
-    scale = 1.0
-    for k in range(args.steps):
+    steps = []
+    for _ in range(args.steps):
         ts = time.perf_counter()
-        v, parts, sample = oracle_estimate(
-            inp, iters, nthreads, target_sample=max(2048, int(65536 * scale)),
-            leaf_sample=10 ** 9 if scale >= 1.0 else max(4, int(600 * scale)),
-            atom_sample=max(16, int(400 * scale)))
-        vals.append(v)
-        if k == 0 and args.steps > 1:
-            w1 = time.perf_counter() - ts
-            scale = min(1.0, max(0.02, (REF_BUDGET_S - w1) / ((args.steps - 1) * w1)))
+        parts, res = oracle_solve(inp, nthreads)
+        steps.append(time.perf_counter() - ts)
     wall = time.perf_counter() - t0
-    value = float(np.mean(vals))
+    value = args.steps / sum(steps)
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 / value, "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "ms_per_step": 1e3 * sum(steps) / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": WORKLOAD_NAME, "faces": len(inp["nvert"]),
-                   "atoms": len(inp["atmchr"]), "gmres_iterations": iters},
+                   "atoms": len(inp["atmchr"]), "gmres_iterations": res["iter"],
+                   "soleng_kcal_mol": res["soleng"]},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": nthreads,
-                         "kind": "port", "sample": sample,
-                         "phase_s": {k: round(x, 4) for k, x in parts.items()}},
+                         "kind": "port",
+                         "sample": "complete solves (form_matrix, tree, DGMRES with the leaf "
+                                   "blocks re-factored on every apply as the reference does, "
+                                   "energy) of the benchmark molecule, every timed step; "
+                                   f"{nthreads} host threads",
+                         "phase_s": {k: round(x, 4) for k, x in parts.items()},
+                         "matvecs": res["n_matvec"], "applies": res["n_msolve"]},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
-        "sample_wall_s": wall,
+        "timed_wall_s": wall,
     }), flush=True)
 
 
@@ -673,9 +680,10 @@ def main():
     ap.add_argument("--batch-workers", type=int, default=4)
     ap.add_argument("--no-large", dest="large", action="store_false",
                     help="skip the large mixed-precision leg (20,000 atoms, order 6, tol 1e-6)")
-    ap.add_argument("--iters", type=int, default=6,
-                    help="GMRES iterations used to scale the reference-arm sample")
     ap.add_argument("--workload", choices=sorted(WORKLOADS), default="globular")
+    ap.add_argument("--pivoted-lu", action="store_true",
+                    help="factor every leaf block with partial pivoting (TABI_FLAG_PIVOTED_LU) "
+                         "in the main leg, instead of the certified unpivoted factorisation")
     args = ap.parse_args()
     global WORKLOAD, WORKLOAD_NAME
     WORKLOAD = WORKLOADS[args.workload]

@@ -164,7 +164,10 @@ int tabi_energy_dev(tabi_h h, int nchr, const double* chrpos_dev,
  * x (2 nface, same face order), atoms (chrpos 3 x nchr, atmchr); out receives
  * [soleng, couleng] (kcal/mol).  nchr <= 524288, else TABI_ERR_LIMIT.  The
  * first call on a device looks up the scratch address (cudaGetSymbolAddress)
- * and should come before any stream capture.  Every call writes the scratch
+ * and should come before any stream capture.  The address is cached for the
+ * life of the process: do not call this after cudaDeviceReset (or anything
+ * else that recreates the device's primary context), which reloads the module
+ * at another address.  Every call writes the scratch
  * it reads, nothing needs clearing; calls that overlap on the GPU (on
  * different streams) share the scratch and race. */
 int tabi_energy_noalloc(int nface, const double* tr_xyz_dev,

@@ -43,7 +43,7 @@ def lib():
         L.or_surface_area.argtypes = [C.c_int, _dp, C.c_int, _ip, C.POINTER(C.c_double)]
         L.or_surface_area.restype = C.c_int
         L.or_form_matrix.argtypes = [C.c_int, _dp, _dp, C.c_int, _ip, C.c_int, _dp, _dp,
-                                     C.c_double, _dp, _dp, _dp, _dp]
+                                     C.c_double, _dp, _dp, _dp, _dp, C.c_int]
         L.or_form_matrix.restype = None
         L.or_tree_create.argtypes = [C.c_int, _dp, _dp, _dp, C.c_void_p, C.c_int, C.c_int,
                                      C.c_double, _ip, C.POINTER(C.c_int)]
@@ -111,7 +111,7 @@ def surface_area(sptpos, nvert):
     return nv[:nnew].copy(), s.value
 
 
-def form_matrix(sptpos, sptnrm, nvert, chrpos, atmchr, eps0):
+def form_matrix(sptpos, sptnrm, nvert, chrpos, atmchr, eps0, nthreads=1):
     """main.f90:546-610.  Returns tr_xyz (N,3), tr_q (N,3), tr_area (N,), bvct (2N,)."""
     sp = _d(sptpos).reshape(-1, 3)
     sn = _d(sptnrm).reshape(-1, 3)
@@ -124,7 +124,8 @@ def form_matrix(sptpos, sptnrm, nvert, chrpos, atmchr, eps0):
     ar = np.zeros(n)
     b = np.zeros(2 * n)
     lib().or_form_matrix(sp.shape[0], sp.ravel(), sn.ravel(), n, nv.ravel(), cp.shape[0],
-                         cp.ravel(), q, float(eps0), xyz.ravel(), tq.ravel(), ar, b)
+                         cp.ravel(), q, float(eps0), xyz.ravel(), tq.ravel(), ar, b,
+                         int(nthreads))
     return xyz, tq, ar, b
 
 
@@ -212,7 +213,9 @@ class Tree:
         x = np.zeros_like(b) if x0 is None else _d(x0).ravel().copy()
         it = C.c_int()
         err = C.c_double()
-        hist = np.zeros((nrmax + 1) * maxl + 2)
+        # DGMRES reads MAXL 0 as 10, NRMAX 0 as 10 and NRMAX -1 as no restart
+        cap = ({0: 10, -1: 0}.get(nrmax, nrmax) + 1) * (maxl or 10)
+        hist = np.zeros(cap + 2)
         nh = C.c_int()
         nmv = np.zeros(1, np.int64)
         nms = np.zeros(1, np.int64)

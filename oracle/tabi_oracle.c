@@ -95,11 +95,13 @@ void or_form_matrix(int nspt, const double* sptpos, const double* sptnrm,
                     int nface, const int* nvert, int nchr,
                     const double* chrpos, const double* atmchr, double eps0,
                     double* tr_xyz, double* tr_q, double* tr_area,
-                    double* bvct) {
+                    double* bvct, int nthreads) {
   (void)nspt;
   const double pi = PI_F;
   const double third = 1.0 / 3.0;
   for (int i = 0; i < 2 * nface; ++i) bvct[i] = 0.0;
+  /* faces are independent: threads change nothing in the results */
+#pragma omp parallel for num_threads(nthreads > 0 ? nthreads : 1) schedule(static)
   for (int i = 0; i < nface; ++i) {
     double r0[3] = {0, 0, 0}, v0[3] = {0, 0, 0}, r[3][3];
     for (int k = 0; k < 3; ++k) {

@@ -38,7 +38,7 @@ void or_form_matrix(int nspt, const double* sptpos, const double* sptnrm,
                     int nface, const int* nvert, int nchr,
                     const double* chrpos, const double* atmchr, double eps0,
                     double* tr_xyz, double* tr_q, double* tr_area,
-                    double* bvct);
+                    double* bvct, int nthreads);
 
 /* main.f90:329-464 treecode_initialization: SETUP + CREATE_TREE (with the
  * reference's in-place PARTITION, so orderarr matches the reference's), then

@@ -226,6 +226,10 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
   // DGMRES :754-781: BNRM = |M^-1 b|, r = b - A x
   msolve_dev(H, b, r, s);
   double bnrm = nrm2_dev(H, r, n, s);
+  // the reference would iterate on NaNs to the iteration limit; a non-finite
+  // right-hand side is refused instead
+  TABI_REQUIRE(std::isfinite(bnrm), TABI_ERR_ARG,
+               "the right-hand side is not finite (|M^-1 b| is NaN or Inf)");
   matvec_dev(H, x, r, s, true);
   { TABI_K(K_VEC, s); sub_kernel<<<vb, vt, 0, s>>>(n, b, r); }
   for (;;) {
@@ -243,6 +247,8 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
     }
     TABI_CUDA(cudaMemcpyAsync(Vc(1), r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     double r0nrm = nrm2_dev(H, Vc(1), n, s);
+    TABI_REQUIRE(nrsts > 0 || std::isfinite(r0nrm), TABI_ERR_ARG,
+                 "the initial residual is not finite (x0 holds NaN or Inf)");
     err = r0nrm / bnrm;  // ISDGMR with LGMR = 0
     bool zero_z = true;
     if (!(err <= tol)) {
@@ -427,6 +433,8 @@ void solve_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
   const int vb = kVecBlocks, vt = 256;
   msolve_dev(H, b, t, s);
   const double bnrm = nrm2_dev(H, t, n, s);
+  TABI_REQUIRE(std::isfinite(bnrm), TABI_ERR_ARG,
+               "the right-hand side is not finite (|M^-1 b| is NaN or Inf)");
   std::vector<double> inner_hist((size_t)cap + 1);
   int iter = 0, ierr = 0, nh = 0;
   double err = 0.0;
@@ -438,6 +446,8 @@ void solve_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
     { TABI_K(K_VEC, s); sub_kernel<<<vb, vt, 0, s>>>(n, b, r); }
     msolve_dev(H, r, t, s);
     err = nrm2_dev(H, t, n, s) / bnrm;
+    TABI_REQUIRE(outer > 0 || std::isfinite(err), TABI_ERR_ARG,
+                 "the initial residual is not finite (x0 holds NaN or Inf)");
     if (err <= tol) {
       ierr = 0;
       break;

@@ -13,7 +13,10 @@
 //
 // Host code only ever sees a host-side stand-in for that symbol, so the device
 // address is looked up with cudaGetSymbolAddress once per device (on the first
-// call made with that device current) and passed to the kernels.
+// call made with that device current) and passed to the kernels.  The cached
+// address stays valid only while the device's primary context lives: a
+// cudaDeviceReset reloads the module elsewhere, so callers must not reset the
+// device between calls (the header says so).
 #include <cmath>
 #include <mutex>
 

@@ -105,8 +105,9 @@ __global__ void __launch_bounds__(kLuThreads) lu_kernel(const int2* __restrict__
     // ---- panel factorization (columns k0 .. k0+nb-1)
     for (int kk = k0; kk < k0 + nb; ++kk) {
       double* col = A + (size_t)kk * m;
+      // a column of NaNs offers no candidate: the diagonal row stays the pivot
       double bv = -1.0;
-      int bi = m;
+      int bi = kk;
       for (int i = kk + tid; i < m; i += blockDim.x) argmax_merge(bv, bi, fabs(col[i]), i);
       for (int o = 16; o > 0; o >>= 1) {
         double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -277,8 +278,9 @@ __device__ void panel_factor(double* P, int mr, int r0, int nb, int k0, int* ip,
   for (int j = 0; j < nb; ++j) {
     const int lr0 = r0 + j;  // local row of the diagonal
     double* col = P + (size_t)j * mr;
+    // a column of NaNs offers no candidate: the diagonal row stays the pivot
     double bv = -1.0;
-    int bi = mr;
+    int bi = lr0;
     for (int i = lr0 + tid; i < mr; i += kPT) argmax_merge(bv, bi, fabs(col[i]), i);
     for (int o = 16; o > 0; o >>= 1) {
       double v2 = __shfl_xor_sync(0xffffffffu, bv, o);
@@ -1011,7 +1013,8 @@ __global__ void lu_diaginv_kernel(const int2* __restrict__ blocks,  // (leaf, k0
                                   const int2* __restrict__ leaf_rng,
                                   const int64_t* __restrict__ blk_off,
                                   const int64_t* __restrict__ dinv_off,
-                                  const double* __restrict__ lu, double* __restrict__ dinv) {
+                                  const double* __restrict__ lu, double* __restrict__ dinv,
+                                  int* __restrict__ info) {
   __shared__ double D[4][kDB][kDB + 1];
   int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
   int2 bk = blocks[blockIdx.x * 4 + w];
@@ -1023,6 +1026,9 @@ __global__ void lu_diaginv_kernel(const int2* __restrict__ blocks,  // (leaf, k0
     D[w][lane][c] = (c < nb && lane < nb) ? A[(size_t)(k0 + c) * m + k0 + lane]
                                           : (c == lane ? 1.0 : 0.0);
   __syncwarp();
+  // a NaN or Inf pivot (coincident faces give a non-finite kernel value) is
+  // recorded as -(its 1-based row); DGETRF's exact-zero info takes precedence
+  if (lane < nb && !isfinite(D[w][lane][lane])) atomicCAS(&info[bk.x], 0, -(k0 + lane + 1));
   double* Li = dinv + dinv_off[bk.x] + (size_t)(k0 / kDB) * 2 * kDB * kDB;
   double* Ui = Li + kDB * kDB;
   // L^{-1} e_j (unit lower)
@@ -1465,14 +1471,6 @@ void build_precond(Handle& H, cudaStream_t s) {
                                           d_info.p, kPanelMaxM);
     }
   }
-  std::vector<int> info(nl);
-  TABI_CUDA(cudaMemcpyAsync(info.data(), d_info.p, sizeof(int) * nl, cudaMemcpyDeviceToHost, s));
-  TABI_CUDA(cudaStreamSynchronize(s));
-  for (int l = 0; l < nl; ++l)
-    if (info[l] != 0)
-      throw Error(TABI_ERR_SINGULAR, "leaf block " + std::to_string(l) +
-                                         " is singular (DGETRF info " +
-                                         std::to_string(info[l]) + ")");
   // pivot permutations and inverse diagonal blocks for the applies
   {
     T.dinv_off.resize(nl);
@@ -1496,7 +1494,25 @@ void build_precond(Handle& H, cudaStream_t s) {
                               cudaMemcpyHostToDevice, s));
     { TABI_K(K_LU_POST, s); lu_perm_kernel<<<ceil_div(nl, 64), 64, 0, s>>>(T.d_leaf_rng.p, T.d_piv.p, nl, T.d_lu_perm.p); }
     { TABI_K(K_LU_POST, s); lu_diaginv_kernel<<<(int)(dblocks.size() / 4), 128, 0, s>>>(
-        H.pc_dblocks.p, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_lu.p, T.d_dinv.p); }
+        H.pc_dblocks.p, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_lu.p, T.d_dinv.p,
+        d_info.p); }
+  }
+  {
+    std::vector<int> info(nl);
+    TABI_CUDA(cudaMemcpyAsync(info.data(), d_info.p, sizeof(int) * nl, cudaMemcpyDeviceToHost,
+                              s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+    for (int l = 0; l < nl; ++l) {
+      if (info[l] > 0)
+        throw Error(TABI_ERR_SINGULAR, "leaf block " + std::to_string(l) +
+                                           " is singular (DGETRF info " +
+                                           std::to_string(info[l]) + ")");
+      if (info[l] < 0)
+        throw Error(TABI_ERR_SINGULAR, "leaf block " + std::to_string(l) +
+                                           " has a non-finite pivot at row " +
+                                           std::to_string(-info[l]) +
+                                           " (coincident faces or non-finite surface data)");
+    }
   }
   // apply lists: blocks of order > 512 get 512 threads (one wave on the GPU),
   // the others 256 threads on the side stream; largest first in each

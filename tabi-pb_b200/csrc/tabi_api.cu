@@ -49,9 +49,11 @@ int guarded(tabi_h h, F&& f) {
     return e.code;
   } catch (const std::bad_alloc&) {
     if (h) h->H.err = "host allocation failed";
+    g_err = "host allocation failed";
     return TABI_ERR_NOMEM;
   } catch (const std::exception& e) {
     if (h) h->H.err = e.what();
+    g_err = e.what();
     return TABI_ERR_CUDA;
   }
 }
@@ -151,11 +153,22 @@ void require_tree(Handle& H, int n2) {
   TABI_REQUIRE(n2 == 2 * H.n, TABI_ERR_ARG, "vector length must be 2*nface");
 }
 
+// the preconditioner factors with the tree: a tree whose leaf blocks cannot be
+// factored (TABI_ERR_SINGULAR) leaves the handle without a tree
+void precond_or_reset(Handle& H, cudaStream_t s) {
+  try {
+    build_precond(H, s);
+  } catch (...) {
+    H.has_tree = H.has_precond = false;
+    throw;
+  }
+}
+
 void do_build(Handle& H, cudaStream_t s) {
   build_tree(H, s);
   build_lists(H, s);
   H.has_tree = true;
-  build_precond(H, s);
+  precond_or_reset(H, s);
 }
 
 template <typename T>
@@ -216,7 +229,7 @@ void run_molecule(Handle& H, WsNet* ws, const MolDev& m, double* x_dev, double* 
   build_lists(H, s);
   H.has_tree = true;
   mark("lists");
-  build_precond(H, s);
+  precond_or_reset(H, s);
   mark("precond");
   { TABI_K(K_FORM, s); permute_b_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(H.d_perm.p, nface, b0.p, b.p); }
   DBuf<double>& xl = H.rn_x;

@@ -171,7 +171,10 @@ class TabiSolver:
             x[:] = 0.0 if x0 is None else f64(x0).ravel()
         it, ierr, nh = C.c_int(), C.c_int(), C.c_int()
         err = C.c_double()
-        hist = np.zeros((self.params.nrmax + 1) * max(self.params.maxl, 1) + 2)
+        # DGMRES reads MAXL 0 as 10, NRMAX 0 as 10 and NRMAX -1 as no restart
+        maxl = self.params.maxl or 10
+        nrmax = {0: 10, -1: 0}.get(self.params.nrmax, self.params.nrmax)
+        hist = np.zeros((nrmax + 1) * maxl + 2)
         check(self.h, self.L.tabi_solve(self.h, b.size, dptr(b), dptr(x), C.byref(it),
                                         C.byref(err), C.byref(ierr), dptr(hist), C.byref(nh)))
         return dict(x=x, iter=it.value, err=err.value, ierr=ierr.value,

@@ -55,6 +55,9 @@ CASES = {
     "mol60_p6_L100": (lambda: molecule_case(60, 6.0, 2.0, seed=4), dict(maxparnode=100, order=6,
                                                                          theta=0.7)),
     "born_l3_p8_L100": (lambda: born_case(3), dict(maxparnode=100, order=8, theta=0.6)),
+    # MSOLVEprec (main.f90:532-542): diagonal scaling instead of the leaf blocks
+    "mol60_L200_iprcd0": (lambda: molecule_case(60, 6.0, 2.0, seed=1), dict(maxparnode=200,
+                                                                             iprcd=0)),
 }
 
 
@@ -63,6 +66,7 @@ def setup(request, gpu_lib):
     mk, kw = CASES[request.param]
     case = mk()
     s, T, kap, g, o = _setup(case, **kw)
+    T.iprcd = kw.get("iprcd", 1)
     yield request.param, case, s, T, kap, g, o
     s.close()
 
@@ -141,8 +145,8 @@ def test_msolve(setup):
     rng = np.random.default_rng(11)
     r = rng.normal(size=2 * n)
     zg = _from_tree(s.msolve(_to_tree(r, s.orderarr, n)), s.orderarr, n)
-    zo = _from_tree(T.msolve(kap, EPS1 / EPS0, _to_tree(r, T.orderarr, n), nthreads=8),
-                    T.orderarr, n)
+    zo = _from_tree(T.msolve(kap, EPS1 / EPS0, _to_tree(r, T.orderarr, n), iprcd=T.iprcd,
+                             nthreads=8), T.orderarr, n)
     rel = np.linalg.norm(zg - zo) / np.linalg.norm(zo)
     assert rel < MATVEC_TOL, rel
 
@@ -153,7 +157,7 @@ def test_solve_and_energy(setup):
     _, _, _, b = g
     bt = _to_tree(b, s.orderarr, n)
     res = s.dgmres(bt)
-    ores = T.dgmres(kap, EPS1 / EPS0, T.bvct, iprcd=1, tol=1e-4, nthreads=8)
+    ores = T.dgmres(kap, EPS1 / EPS0, T.bvct, iprcd=T.iprcd, tol=1e-4, nthreads=8)
     assert res["ierr"] == ores["ierr"] == 0
     assert res["iter"] == ores["iter"]
     np.testing.assert_allclose(res["err_hist"], ores["err_hist"], rtol=1e-8)
