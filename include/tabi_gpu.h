@@ -68,8 +68,17 @@ typedef struct {
   int maxl;        /* GMRES restart length (reference: 10) */
   int nrmax;       /* max restarts (reference: 10) */
   int precision;   /* TABI_PREC_* */
-  int flags;       /* reserved, 0 */
+  int flags;       /* TABI_FLAG_* bits, 0 for the defaults */
 } tabi_params;
+
+/* The leaf blocks are factored by a blocked LU without row interchanges whose
+ * every multiplier is checked against |l| <= 1 - 2^-20: when that holds,
+ * DGETRF2's partial pivoting (treecode3d_pb.f:1530, dgetrf_dep.f:757-900)
+ * keeps the diagonal row at every column and the factors are its factors;
+ * a leaf that fails the check is factored again with partial pivoting.  This
+ * flag factors every leaf with partial pivoting from the start (the same
+ * factors, slower). */
+#define TABI_FLAG_PIVOTED_LU 1
 
 /* Fills p with the reference defaults: order 3, maxparnode 500, theta 0.8,
  * eps 1/80, 0.15 M (kappa from tabi_kappa), iprcd 1, tol 1e-4, maxl 10,
@@ -192,6 +201,11 @@ int tabi_run_dev(tabi_h h, int nspt, const double* sptpos_dev,
  * far-field (target, cluster) evaluations; as the reference's traversal
  * would perform them. */
 int tabi_counts(tabi_h h, int64_t* near_pairs, int64_t* far_interactions);
+
+/* Leaf blocks of the current tree that were factored with partial pivoting:
+ * those whose no-interchange check failed (see TABI_FLAG_PIVOTED_LU), or all
+ * of them when that flag is set.  No counterpart in the reference. */
+int tabi_pivoted_leaves(tabi_h h, int* count);
 
 /* Node table of the current tree in depth-first (reference creation) order:
  * ibeg (1-based), numpar, level, num_children, and geo = x_mid, y_mid,

@@ -14,6 +14,8 @@
 // never changes, so here it is assembled and factored once per tree
 // (right-looking LU with partial pivoting, the same pivot rule, batched over
 // all leaves) and every apply is a blocked forward/back substitution.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <climits>
 
@@ -81,13 +83,14 @@ __device__ __forceinline__ void argmax_merge(double& v, int& i, double v2, int i
 // Right-looking blocked LU with partial pivoting of one leaf block per CTA,
 // panel in global memory (used for blocks too large for the shared-memory
 // panel of the batched kernels).
-__global__ void __launch_bounds__(kLuThreads) lu_kernel(const int2* __restrict__ leaf_rng,
+__global__ void __launch_bounds__(kLuThreads) lu_kernel(const int* __restrict__ leaves,
+                                                        const int2* __restrict__ leaf_rng,
                                                         const int64_t* __restrict__ blk_off,
                                                         double* __restrict__ lu,
                                                         int* __restrict__ piv,
                                                         int* __restrict__ info,
                                                         int skip_max_m) {
-  int leaf = blockIdx.x;
+  int leaf = leaves[blockIdx.x];
   int2 lr = leaf_rng[leaf];
   int m = 2 * lr.y;
   if (m <= skip_max_m) return;  // factored by the batched kernels
@@ -1234,6 +1237,445 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
   }
 }
 
+// ---------------------------------------------------------------------------
+// Unpivoted blocked LU with a certificate of partial pivoting.
+//
+// DGETRF2 swaps rows only where a column holds an entry larger in magnitude
+// than its diagonal after elimination (IDAMAX, first index on ties).  The leaf
+// blocks of a well-resolved surface are strongly diagonal (the 2n x 2n blocks
+// of the benchmark molecule have condition numbers near 100 and no row
+// interchange at all), so the factorisation runs first without pivot
+// searches, as a right-looking blocked LU in 64-column steps:
+//   lu_np_diag_kernel   the 64 x 64 diagonal block of every leaf, factored in
+//                       shared memory, with the inverses of its L and U
+//                       (kept for the panels, and their 32 x 32 diagonal
+//                       blocks for the applies);
+//   lu_np_panel_kernel  L21 = A21 U11^{-1} by 64-row chunks and
+//                       U12 = L11^{-1} A12 by 64-column chunks;
+//   lu_gemm2_kernel     A22 -= L21 U12, 64 deep.
+// Every multiplier l is checked: |l| <= 1 - 2^-20 for all of them certifies
+// that partial pivoting (on these values or on the reference's, which differ
+// by rounding only) keeps the diagonal row at every column, so the factors
+// are DGETRF's.  A leaf whose certificate fails anywhere (a larger entry, a
+// near tie, a zero or non-finite pivot) is re-assembled and factored again by
+// the pivoted kernels above.
+constexpr int kNP = 64;    // step width
+constexpr int kNPT = 256;  // threads of the diagonal and panel kernels
+constexpr int kNPPitch = kNP + 1;
+constexpr double kNoPivBound = 1.0 - 1.0 / 1048576.0;
+constexpr size_t kNPDiagSmem = sizeof(double) * 3 * kNP * kNPPitch;
+constexpr size_t kNPPanelSmem = sizeof(double) * 2 * kNP * kNPPitch;
+
+// Per leaf (leaves[blockIdx.x]) with m > k0: D = A[k0:k0+d, k0:k0+d], d =
+// min(64, m - k0), factored in place without interchanges (DGETRF2's scaling:
+// reciprocal unless the pivot is below the smallest normal); scr receives
+// L^{-1} (unit lower) and U^{-1} of D (64 x 64 each, column-major, zeros
+// outside the triangle), dinv the 32 x 32 diagonal blocks of both (identity
+// padded), the layout lu_diaginv_kernel writes.
+__global__ void __launch_bounds__(kNPT) lu_np_diag_kernel(
+    const int* __restrict__ leaves, int k0, const int2* __restrict__ leaf_rng,
+    const int64_t* __restrict__ blk_off, const int64_t* __restrict__ dinv_off,
+    double* __restrict__ lu, double* __restrict__ dinv, double* __restrict__ scr,
+    int* __restrict__ fail) {
+  extern __shared__ double nsm[];
+  double(*D)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm);
+  double(*Li)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm + kNP * kNPPitch);
+  double(*Ui)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm + 2 * kNP * kNPPitch);
+  const int leaf = leaves[blockIdx.x];
+  const int m = 2 * leaf_rng[leaf].y;
+  const int d = min(kNP, m - k0);
+  double* A = lu + blk_off[leaf];
+  const int tid = threadIdx.x;
+  for (int e = tid; e < d * d; e += kNPT) {
+    const int c = e / d, r = e - c * d;
+    D[r][c] = A[(size_t)(k0 + c) * m + k0 + r];
+  }
+  __syncthreads();
+  bool bad = false;
+  for (int j = 0; j < d; ++j) {
+    const double pk = D[j][j];
+    if (!(pk != 0.0 && isfinite(pk))) bad = true;
+    const bool recip = fabs(pk) >= 2.2250738585072014e-308;
+    const double rcp = 1.0 / pk;
+    if (tid > j && tid < d) {
+      const double l = recip ? D[tid][j] * rcp : D[tid][j] / pk;
+      if (!(fabs(l) <= kNoPivBound)) bad = true;
+      D[tid][j] = l;
+    }
+    __syncthreads();
+    const int w = d - 1 - j;
+    for (int e = tid; e < w * w; e += kNPT) {
+      const int i = j + 1 + e % w, c = j + 1 + e / w;
+      D[i][c] = fma(-D[i][j], D[j][c], D[i][c]);
+    }
+    __syncthreads();
+  }
+  // inverses, one column per thread: threads 0..d-1 L^{-1}, 64..64+d-1 U^{-1}
+  if (tid < d) {
+    const int c = tid;
+    for (int i = 0; i < kNP; ++i) Li[i][c] = 0.0;
+    Li[c][c] = 1.0;
+    for (int i = c + 1; i < d; ++i) {
+      double v0 = 0.0, v1 = 0.0;
+      int q = c;
+      for (; q + 1 < i; q += 2) {
+        v0 = fma(-D[i][q], Li[q][c], v0);
+        v1 = fma(-D[i][q + 1], Li[q + 1][c], v1);
+      }
+      if (q < i) v0 = fma(-D[i][q], Li[q][c], v0);
+      Li[i][c] = v0 + v1;
+    }
+  } else if (tid >= kNP && tid < kNP + d) {
+    const int c = tid - kNP;
+    for (int i = 0; i < kNP; ++i) Ui[i][c] = 0.0;
+    Ui[c][c] = 1.0 / D[c][c];
+    for (int i = c - 1; i >= 0; --i) {
+      double v0 = 0.0, v1 = 0.0;
+      int q = i + 1;
+      for (; q + 1 <= c; q += 2) {
+        v0 = fma(-D[i][q], Ui[q][c], v0);
+        v1 = fma(-D[i][q + 1], Ui[q + 1][c], v1);
+      }
+      if (q <= c) v0 = fma(-D[i][q], Ui[q][c], v0);
+      Ui[i][c] = (v0 + v1) / D[i][i];
+    }
+  }
+  if (__syncthreads_or(bad) && tid == 0) fail[leaf] = 1;
+  // factors back, inverses out
+  for (int e = tid; e < d * d; e += kNPT) {
+    const int c = e / d, r = e - c * d;
+    A[(size_t)(k0 + c) * m + k0 + r] = D[r][c];
+  }
+  double* S = scr + (size_t)blockIdx.x * 2 * kNP * kNP;
+  for (int e = tid; e < kNP * kNP; e += kNPT) {
+    const int c = e / kNP, r = e - c * kNP;
+    S[e] = (r < d && c < d) ? Li[r][c] : 0.0;
+    S[kNP * kNP + e] = (r < d && c < d) ? Ui[r][c] : 0.0;
+  }
+  double* Di = dinv + dinv_off[leaf] + (size_t)(k0 / kDB) * 2 * kDB * kDB;
+  for (int b = 0; b * kDB < d; ++b) {
+    const int nb = min(kDB, d - b * kDB), o = b * kDB;
+    double* Lb = Di + (size_t)b * 2 * kDB * kDB;
+    double* Ub = Lb + kDB * kDB;
+    for (int e = tid; e < kDB * kDB; e += kNPT) {
+      const int c = e / kDB, r = e - c * kDB;
+      const double id = r == c ? 1.0 : 0.0;
+      Lb[e] = (r < nb && c < nb) ? Li[o + r][o + c] : id;
+      Ub[e] = (r < nb && c < nb) ? Ui[o + r][o + c] : id;
+    }
+  }
+}
+
+// item = (leaf, slot, kind, off): kind 0, rows [off, off + 64) of the step's
+// column panel: L21 = A21 U11^{-1}, each multiplier checked; kind 1, columns
+// [off, off + 64) of its row panel: U12 = L11^{-1} A12.  slot = the leaf's
+// row in the diagonal kernel's launch (its scratch).
+__global__ void __launch_bounds__(kNPT) lu_np_panel_kernel(
+    const int4* __restrict__ items, int k0, const int2* __restrict__ leaf_rng,
+    const int64_t* __restrict__ blk_off, double* __restrict__ lu,
+    const double* __restrict__ scr, int* __restrict__ fail) {
+  extern __shared__ double nsm[];
+  double(*X)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm);
+  double(*V)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm + kNP * kNPPitch);
+  const int4 it = items[blockIdx.x];
+  const int leaf = it.x, kind = it.z, off = it.w;
+  const int m = 2 * leaf_rng[leaf].y;
+  const int d = min(kNP, m - k0);
+  const int cnt = min(kNP, m - off);
+  double* A = lu + blk_off[leaf];
+  const double* S = scr + (size_t)it.y * 2 * kNP * kNP + (kind == 0 ? kNP * kNP : 0);
+  const int tid = threadIdx.x;
+  // V[a][b] = the inverse (L^{-1} or U^{-1}), zeros outside d x d
+  for (int e = tid; e < kNP * kNP; e += kNPT) {
+    const int c = e / kNP, r = e - c * kNP;
+    V[r][c] = S[e];
+  }
+  bool bad = false;
+  if (kind == 0) {
+    // X[i][q] = A[off + i, k0 + q]
+    for (int e = tid; e < kNP * kNP; e += kNPT) {
+      const int q = e / kNP, i = e - q * kNP;
+      X[i][q] = (i < cnt && q < d) ? A[(size_t)(k0 + q) * m + off + i] : 0.0;
+    }
+    __syncthreads();
+    const int i = tid % kNP, c0 = (tid / kNP) * 16;
+    double acc[16];
+#pragma unroll
+    for (int cc = 0; cc < 16; ++cc) acc[cc] = 0.0;
+    for (int q = 0; q < d; ++q) {
+      const double x = X[i][q];
+#pragma unroll
+      for (int cc = 0; cc < 16; ++cc) acc[cc] = fma(x, V[q][c0 + cc], acc[cc]);
+    }
+    if (i < cnt) {
+#pragma unroll
+      for (int cc = 0; cc < 16; ++cc) {
+        const int c = c0 + cc;
+        if (c < d) {
+          if (!(fabs(acc[cc]) <= kNoPivBound)) bad = true;
+          A[(size_t)(k0 + c) * m + off + i] = acc[cc];
+        }
+      }
+    }
+  } else {
+    // X[q][c] = A[k0 + q, off + c]
+    for (int e = tid; e < kNP * kNP; e += kNPT) {
+      const int c = e / kNP, q = e - c * kNP;
+      X[q][c] = (c < cnt && q < d) ? A[(size_t)(off + c) * m + k0 + q] : 0.0;
+    }
+    __syncthreads();
+    const int c = tid % kNP, r0 = (tid / kNP) * 16;
+    double acc[16];
+#pragma unroll
+    for (int rr = 0; rr < 16; ++rr) acc[rr] = 0.0;
+    for (int q = 0; q < d; ++q) {
+      const double x = X[q][c];
+#pragma unroll
+      for (int rr = 0; rr < 16; ++rr) acc[rr] = fma(V[r0 + rr][q], x, acc[rr]);
+    }
+    if (c < cnt) {
+#pragma unroll
+      for (int rr = 0; rr < 16; ++rr)
+        if (r0 + rr < d) A[(size_t)(off + c) * m + k0 + r0 + rr] = acc[rr];
+    }
+  }
+  if (__syncthreads_or(bad) && tid == 0) fail[leaf] = 1;
+}
+
+// Trailing update of the unpivoted factorisation: item = (leaf, r0, c0, 0):
+// C = A[r0:r0+128, c0:c0+64] -= A[r0:, k0:k0+kd] A[k0:k0+kd, c0:] with
+// kd = min(64, m - k0), rows and columns clipped at m.  256 threads, 8 x 4
+// outputs each: rows 2 tr + 32 a + {0, 1} (a = 0..3; each pair one 16-byte
+// shared load, eight lanes of a load phase on 32 distinct banks) and columns
+// 4 tc .. 4 tc + 3 (two 16-byte loads, broadcast within a phase).  C is loaded
+// into the accumulators and the products subtracted one k at a time
+// (fma(-l, u, c)), the order of the reference's DGEMM (C := C - A B,
+// dgetrf_dep.f), while the two 32-deep slices of L and U arrive by cp.async
+// (zero-filled outside the tile: m, r0, c0, k0 and the depth are even, so a
+// 16-byte chunk of L is wholly inside or outside; U comes in 8-byte copies,
+// being transposed to k-major).
+constexpr int kG2M = 128, kG2N = 64, kG2K = 32;
+constexpr size_t kGemm2Smem = sizeof(double) * 2 * (kG2K * kG2M + kG2K * kG2N);
+
+__global__ void __launch_bounds__(256, 2) lu_gemm2_kernel(const int4* __restrict__ items, int k0,
+                                                          const int2* __restrict__ leaf_rng,
+                                                          const int64_t* __restrict__ blk_off,
+                                                          double* __restrict__ lu) {
+  extern __shared__ double gsm2[];
+  double* sL = gsm2;                      // [2][kG2K][kG2M]  L slice, k-major
+  double* sU = gsm2 + 2 * kG2K * kG2M;    // [2][kG2K][kG2N]  U slice, k-major
+  const int4 it = items[blockIdx.x];
+  const int leaf = it.x, r0 = it.y, c0 = it.z;
+  const int m = 2 * leaf_rng[leaf].y;
+  const int kd = min(kNP, m - k0);
+  double* A = lu + blk_off[leaf];
+  const int tid = threadIdx.x;
+  const int tr = tid & 15, tc = tid >> 4;
+  auto row_of = [&](int a) { return 2 * tr + 32 * (a >> 1) + (a & 1); };
+  auto load_slice = [&](int kc, int buf) {
+    const int nbk = min(kG2K, kd - kc), kb = k0 + kc;
+    double* L = sL + buf * kG2K * kG2M;
+    double* U = sU + buf * kG2K * kG2N;
+#pragma unroll
+    for (int e = 0; e < (kG2K * kG2M / 2) / 256; ++e) {
+      const int q = tid + 256 * e;
+      const int k = q / (kG2M / 2), rr = 2 * (q % (kG2M / 2));
+      const bool ok = k < nbk && r0 + rr < m;
+      cp_async16(L + k * kG2M + rr, ok ? A + (size_t)(kb + k) * m + r0 + rr : A, ok);
+    }
+#pragma unroll
+    for (int e = 0; e < (kG2K * kG2N / 2) / 256; ++e) {
+      const int q = tid + 256 * e;
+      const int c = q / (kG2K / 2), kk = 2 * (q % (kG2K / 2));
+      const bool ok = kk < nbk && c0 + c < m;
+      const double* src = ok ? A + (size_t)(c0 + c) * m + kb + kk : A;
+      const unsigned d0 = (unsigned)__cvta_generic_to_shared(U + kk * kG2N + c);
+      const unsigned d1 = (unsigned)__cvta_generic_to_shared(U + (kk + 1) * kG2N + c);
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d0), "l"(src),
+                   "r"(ok ? 8 : 0));
+      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d1), "l"(src + 1),
+                   "r"(ok ? 8 : 0));
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  load_slice(0, 0);
+  if (kG2K < kd) load_slice(kG2K, 1);
+  double acc[8][4];
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = c0 + 4 * tc + b;
+    const double* cc = A + (size_t)min(c, m - 1) * m;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int r = r0 + row_of(a);
+      acc[a][b] = (c < m && r < m) ? cc[r] : 0.0;
+    }
+  }
+  for (int kc = 0, buf = 0; kc < kd; kc += kG2K, buf ^= 1) {
+    if (kc + kG2K < kd) {
+      asm volatile("cp.async.wait_group 1;\n" ::);
+    } else {
+      asm volatile("cp.async.wait_group 0;\n" ::);
+    }
+    __syncthreads();
+    const double* L = sL + buf * kG2K * kG2M + 2 * tr;
+    const double* U = sU + buf * kG2K * kG2N + 4 * tc;
+    const int nbk = min(kG2K, kd - kc);
+#pragma unroll 4
+    for (int k = 0; k < nbk; ++k) {
+      const double2 l01 = *reinterpret_cast<const double2*>(L + k * kG2M);
+      const double2 l23 = *reinterpret_cast<const double2*>(L + k * kG2M + 32);
+      const double2 l45 = *reinterpret_cast<const double2*>(L + k * kG2M + 64);
+      const double2 l67 = *reinterpret_cast<const double2*>(L + k * kG2M + 96);
+      const double2 u01 = *reinterpret_cast<const double2*>(U + k * kG2N);
+      const double2 u23 = *reinterpret_cast<const double2*>(U + k * kG2N + 2);
+      const double lv[8] = {l01.x, l01.y, l23.x, l23.y, l45.x, l45.y, l67.x, l67.y};
+      const double uv[4] = {u01.x, u01.y, u23.x, u23.y};
+#pragma unroll
+      for (int a = 0; a < 8; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(-lv[a], uv[b], acc[a][b]);
+    }
+  }
+#pragma unroll
+  for (int b = 0; b < 4; ++b) {
+    const int c = c0 + 4 * tc + b;
+    if (c >= m) continue;
+    double* cc = A + (size_t)c * m;
+#pragma unroll
+    for (int a = 0; a < 8; ++a) {
+      const int r = r0 + row_of(a);
+      if (r < m) cc[r] = acc[a][b];
+    }
+  }
+}
+
+// every leaf: no interchange (1-based local pivots i + 1) and the identity
+// row permutation of the applies
+__global__ void lu_np_identity_kernel(const int2* __restrict__ leaf_rng, int* __restrict__ piv,
+                                      int* __restrict__ perm) {
+  const int2 lr = leaf_rng[blockIdx.x];
+  const int m = 2 * lr.y;
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    piv[2 * lr.x + i] = i + 1;
+    perm[2 * lr.x + i] = i;
+  }
+}
+
+// The apply of a large leaf block (order 512 < m <= 1024) by a cluster of
+// kSC CTAs: the block's 32-row diagonal blocks are split into kSC contiguous
+// runs, one per CTA, and each thread keeps one row of its CTA's run.  Step t
+// of a sweep: the CTA that owns diagonal block t forms y = D_t^{-1} run_t
+// (the inverse staged in its shared memory one step ahead), keeps it, and
+// writes it into every CTA's shared memory (distributed shared memory,
+// double-buffered by step parity); one cluster barrier; every thread then
+// subtracts its row's 32 products with y (the row's 32 factor entries were
+// loaded before the barrier).  Forward sweep L y = P r over the diagonal
+// blocks in order (rows below each step), backward U x = y in reverse order
+// (rows above).  Each SM streams a quarter of the block's factors, instead of
+// one SM all of it.
+constexpr int kSC = 4;      // CTAs per cluster
+constexpr int kSCT = 256;   // threads per CTA (rows per CTA <= 256: m <= 1024)
+
+__global__ void __cluster_dims__(kSC, 1, 1) __launch_bounds__(kSCT) solve_cluster_kernel(
+    const int2* __restrict__ leaf_rng, const int64_t* __restrict__ blk_off,
+    const int64_t* __restrict__ dinv_off, const int* __restrict__ leaf_list,
+    const double* __restrict__ lu, const double* __restrict__ dinv,
+    const int* __restrict__ perm, int N, const double* __restrict__ r,
+    double* __restrict__ z) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const int rank = (int)cl.block_rank();
+  __shared__ double xs[kSCT];          // forward: running values; backward: results
+  __shared__ double fs[kSCT];          // forward: results; backward: running values
+  __shared__ double ybuf[2][kDB];      // the step's 32 values, by step parity
+  __shared__ __align__(16) double dbuf[2][kDB * kDB];
+  const int leaf = leaf_list[blockIdx.x / kSC];
+  const int2 lr = leaf_rng[leaf];
+  const int n = lr.y, m = 2 * n, ib = lr.x;
+  const int nblk = (m + kDB - 1) / kDB;
+  auto first_block = [&](int c) { return (c * nblk) / kSC; };
+  auto owner = [&](int b) {  // the rank whose run holds diagonal block b
+    int c = 0;
+    while (c + 1 < kSC && first_block(c + 1) <= b) ++c;
+    return c;
+  };
+  const int R0 = kDB * first_block(rank), R1 = min(m, kDB * first_block(rank + 1));
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int i = R0 + tid;             // this thread's row
+  const bool mine = i < R1;
+  const double* A = lu + blk_off[leaf];
+  const double* Di = dinv + dinv_off[leaf];
+  if (mine) {
+    const int src = perm[2 * ib + i];
+    xs[tid] = src < n ? r[ib + src] : r[N + ib + src - n];
+  }
+  // the inverse diagonal block of sweep step s (L blocks 0..nblk-1, then U
+  // blocks nblk-1..0) into dbuf[s & 1], by its owner
+  auto block_of = [&](int st) { return st < nblk ? st : 2 * nblk - 1 - st; };
+  auto stage = [&](int st) {
+    if (st >= 2 * nblk || owner(block_of(st)) != rank) return;
+    const int b = block_of(st);
+    const double* src = Di + (size_t)b * 2 * kDB * kDB + (st < nblk ? 0 : kDB * kDB);
+    for (int e = 2 * tid; e < kDB * kDB; e += 2 * kSCT) {
+      const unsigned d = (unsigned)__cvta_generic_to_shared(&dbuf[st & 1][e]);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + e));
+    }
+    asm volatile("cp.async.commit_group;\n" ::);
+  };
+  stage(0);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+  for (int st = 0; st < 2 * nblk; ++st) {
+    const bool fwd = st < nblk;
+    const int b = block_of(st), k0 = b * kDB, nb = min(kDB, m - k0);
+    double* run = fwd ? xs : fs;   // running values of this sweep
+    double* res = fwd ? fs : xs;   // its results
+    // this row's factor entries of the step: L below the block (forward),
+    // U above it (backward)
+    const bool upd = mine && (fwd ? i >= k0 + nb : i < k0);
+    double av[kDB];
+#pragma unroll
+    for (int q = 0; q < kDB; ++q)
+      av[q] = (upd && q < nb) ? A[(size_t)(k0 + q) * m + i] : 0.0;
+    stage(st + 1);
+    if (owner(b) == rank && warp == 0) {
+      const double* D = dbuf[st & 1];
+      double v0 = 0.0, v1 = 0.0;
+      for (int q = 0; q < nb; q += 2) {
+        v0 = fma(D[q * kDB + lane], run[k0 - R0 + q], v0);
+        if (q + 1 < nb) v1 = fma(D[(q + 1) * kDB + lane], run[k0 - R0 + q + 1], v1);
+      }
+      const double y = lane < nb ? v0 + v1 : 0.0;
+      if (lane < nb) res[k0 - R0 + lane] = y;
+#pragma unroll
+      for (int c = 0; c < kSC; ++c) {
+        double* yb = cl.map_shared_rank(&ybuf[st & 1][0], c);
+        yb[lane] = y;
+      }
+    }
+    cl.sync();  // y of this step everywhere (release / acquire)
+    if (upd) {
+      const double* y = ybuf[st & 1];
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+      for (int q = 0; q < kDB; q += 4) {
+        s0 = fma(av[q], y[q], s0);
+        s1 = fma(av[q + 1], y[q + 1], s1);
+        s2 = fma(av[q + 2], y[q + 2], s2);
+        s3 = fma(av[q + 3], y[q + 3], s3);
+      }
+      run[tid] -= (s0 + s1) + (s2 + s3);
+    }
+    asm volatile("cp.async.wait_group 0;\n" ::);
+    __syncthreads();
+  }
+  if (mine) {
+    if (i < n) z[ib + i] = xs[tid];
+    else z[N + ib + i - n] = xs[tid];
+  }
+}
+
 __global__ void diag_kernel(const double* r, double* z, int n, double s1, double s2) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
   if (i < n) z[i] = r[i] / s1;
@@ -1280,15 +1722,151 @@ void build_precond(Handle& H, cudaStream_t s) {
                                                     H.d_ny.p, H.d_nz.p, H.d_area.p,
                                                     H.prm.kappa, eps, T.d_lu.p); }
   TABI_CUDA(cudaMemsetAsync(d_info.p, 0, sizeof(int) * nl, s));
-  {
+  // Two leaf groups with plans of their own: blocks of order above
+  // kLuSmallBlock on the handle's stream, the others on its side stream, so
+  // the many short factorisations of small leaves run beside the long chain of
+  // steps of the large ones instead of inside its launches; one fork after the
+  // assembly, one join at the end.
+  auto fork = [&](bool split) {
+    if (!split) return;
+    TABI_CUDA(cudaEventRecord(H.ev_fork, s));
+    TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
+  };
+  auto join = [&](bool split) {
+    if (!split) return;
+    TABI_CUDA(cudaEventRecord(H.ev_join, H.side));
+    TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
+  };
+  // ---- unpivoted factorisation of every leaf, certified (see lu_np_diag_kernel)
+  std::vector<int> pv_leaves;  // leaves factored with partial pivoting
+  const bool try_np = (H.prm.flags & TABI_FLAG_PIVOTED_LU) == 0;
+  if (try_np) {
+    DBuf<int>& d_fail = H.pc_fail;
+    d_fail.alloc(nl);
+    TABI_CUDA(cudaMemsetAsync(d_fail.p, 0, sizeof(int) * nl, s));
+    T.d_lu_perm.alloc(2 * (size_t)H.n);
+    { TABI_K(K_LU_POST, s); lu_np_identity_kernel<<<nl, 256, 0, s>>>(T.d_leaf_rng.p, T.d_piv.p, T.d_lu_perm.p); }
+    // the inverse diagonal blocks are written by the diagonal kernel
+    T.dinv_off.resize(nl);
+    int64_t doff = 0;
+    for (int l = 0; l < nl; ++l) {
+      T.dinv_off[l] = doff;
+      doff += (int64_t)ceil_div(2 * rng[l].y, kDB) * 2 * kDB * kDB;
+    }
+    T.d_dinv.alloc(std::max<int64_t>(doff, 1));
+    T.d_dinv_off.alloc(nl);
+    TABI_CUDA(cudaMemcpyAsync(T.d_dinv_off.p, T.dinv_off.data(), sizeof(int64_t) * nl,
+                              cudaMemcpyHostToDevice, s));
+    raise_smem_limit((const void*)lu_np_diag_kernel, kNPDiagSmem);
+    raise_smem_limit((const void*)lu_np_panel_kernel, kNPPanelSmem);
+    raise_smem_limit((const void*)lu_gemm2_kernel, kGemm2Smem);
+    std::vector<int> grp[2];
+    for (int l = 0; l < nl; ++l) grp[2 * rng[l].y > kLuSmallBlock ? 0 : 1].push_back(l);
+    for (auto& g : grp)
+      std::sort(g.begin(), g.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
+    const bool split = H.side != nullptr && !grp[0].empty() && !grp[1].empty();
+    fork(split);
+    // right-looking, 64-column steps: diagonal blocks, panels, trailing update
+    auto run_np = [&](const std::vector<int>& order, Handle::NpPlan& B, cudaStream_t st) {
+      int gmax = 0;
+      for (int l : order) gmax = std::max(gmax, 2 * rng[l].y);
+      struct Step {
+        int k0, d0, nd, p0, np, g0, ng;
+      };
+      std::vector<Step> steps;
+      std::vector<int> dl;
+      std::vector<int4> pit, git;
+      int max_slots = 1;
+      for (int k0 = 0; k0 < gmax; k0 += kNP) {
+        Step st0{k0, (int)dl.size(), 0, (int)pit.size(), 0, (int)git.size(), 0};
+        int slot = 0;
+        for (int l : order) {
+          const int m = 2 * rng[l].y;
+          if (m <= k0) continue;
+          dl.push_back(l);
+          const int d = std::min(kNP, m - k0);
+          for (int off = k0 + d; off < m; off += kNP) {
+            pit.push_back(make_int4(l, slot, 0, off));
+            pit.push_back(make_int4(l, slot, 1, off));
+          }
+          for (int r0 = k0 + d; r0 < m; r0 += kG2M)
+            for (int c0 = k0 + d; c0 < m; c0 += kG2N) git.push_back(make_int4(l, r0, c0, 0));
+          ++slot;
+        }
+        max_slots = std::max(max_slots, slot);
+        st0.nd = (int)dl.size() - st0.d0;
+        st0.np = (int)pit.size() - st0.p0;
+        st0.ng = (int)git.size() - st0.g0;
+        steps.push_back(st0);
+      }
+      auto up = [&](auto& buf, const auto& v) {
+        buf.alloc(std::max<size_t>(v.size(), 1));
+        if (!v.empty())
+          TABI_CUDA(cudaMemcpyAsync(buf.p, v.data(), sizeof(v[0]) * v.size(),
+                                    cudaMemcpyHostToDevice, st));
+      };
+      up(B.dleaves, dl);
+      up(B.pitems, pit);
+      up(B.gitems, git);
+      B.scr.alloc((size_t)max_slots * 2 * kNP * kNP);
+      for (const Step& q : steps) {
+        { TABI_K(K_LU, st);
+          lu_np_diag_kernel<<<q.nd, kNPT, kNPDiagSmem, st>>>(
+              B.dleaves.p + q.d0, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_lu.p,
+              T.d_dinv.p, B.scr.p, d_fail.p); }
+        if (q.np > 0) {
+          TABI_K(K_LU_STRIP, st);
+          lu_np_panel_kernel<<<q.np, kNPT, kNPPanelSmem, st>>>(
+              B.pitems.p + q.p0, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, B.scr.p,
+              d_fail.p);
+        }
+        if (q.ng > 0) {
+          TABI_K(K_LU_UPDATE, st);
+          lu_gemm2_kernel<<<q.ng, 256, kGemm2Smem, st>>>(B.gitems.p + q.g0, q.k0,
+                                                         T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p);
+        }
+      }
+    };
+    if (!grp[0].empty()) run_np(grp[0], H.pc_np[0], s);
+    if (!grp[1].empty()) run_np(grp[1], H.pc_np[1], split ? H.side : s);
+    join(split);
+    std::vector<int> failed(nl);
+    TABI_CUDA(cudaMemcpyAsync(failed.data(), d_fail.p, sizeof(int) * nl, cudaMemcpyDeviceToHost,
+                              s));
+    TABI_CUDA(cudaStreamSynchronize(s));
+    for (int l = 0; l < nl; ++l)
+      if (failed[l]) pv_leaves.push_back(l);
+    if (!pv_leaves.empty()) {
+      // those blocks again from their kernel values
+      std::vector<int2> ptiles;
+      for (int l : pv_leaves)
+        for (int j = 0; j < rng[l].y; j += kAsmCols) ptiles.push_back(make_int2(l, j));
+      H.pc_tiles2.alloc(ptiles.size());
+      TABI_CUDA(cudaMemcpyAsync(H.pc_tiles2.p, ptiles.data(), sizeof(int2) * ptiles.size(),
+                                cudaMemcpyHostToDevice, s));
+      TABI_K(K_ASSEMBLE, s);
+      assemble_kernel<<<(int)ptiles.size(), 256, 0, s>>>(H.pc_tiles2.p, T.d_leaf_rng.p,
+                                                         T.d_blk_off.p, H.d_x.p, H.d_y.p,
+                                                         H.d_z.p, H.d_nx.p, H.d_ny.p, H.d_nz.p,
+                                                         H.d_area.p, H.prm.kappa, eps, T.d_lu.p);
+    }
+  } else {
+    for (int l = 0; l < nl; ++l) pv_leaves.push_back(l);
+  }
+  H.pc_pv_leaves = (int)pv_leaves.size();
+  if (!pv_leaves.empty()) {
     // batched LU for blocks with m <= kPanelMaxM; the global-memory kernel for
     // larger ones
     int mmax = 0;
     bool any_big = false;
-    for (int l = 0; l < nl; ++l) {
+    std::vector<int> big_leaves;
+    for (int l : pv_leaves) {
       int m = 2 * rng[l].y;
       if (m <= kPanelMaxM) mmax = std::max(mmax, m);
-      else any_big = true;
+      else {
+        any_big = true;
+        big_leaves.push_back(l);
+      }
     }
     if (mmax > 0) {
       size_t smem = sizeof(double) * (size_t)mmax * kSP;
@@ -1301,17 +1879,14 @@ void build_precond(Handle& H, cudaStream_t s) {
     // panel chain of the large ones instead of inside its launches; one fork
     // after the assembly, one join at the end.
     std::vector<int> grp[2];
-    for (int l = 0; l < nl; ++l) {
+    for (int l : pv_leaves) {
       const int m = 2 * rng[l].y;
       if (m <= kPanelMaxM) grp[m > kLuSmallBlock ? 0 : 1].push_back(l);
     }
     for (auto& g : grp)
       std::sort(g.begin(), g.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
     const bool split = H.side != nullptr && !grp[0].empty() && !grp[1].empty();
-    if (split) {
-      TABI_CUDA(cudaEventRecord(H.ev_fork, s));
-      TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
-    }
+    fork(split);
     // Two-level right-looking LU (LAPACK DGETRF order) of one group.  Outer
     // blocks of kOB columns; inside one, 32-column panel steps update only
     // the block's own columns (and swap the columns left of the panel).  After
@@ -1461,16 +2036,15 @@ void build_precond(Handle& H, cudaStream_t s) {
     };
     if (!grp[0].empty()) run_group(grp[0], H.pc_plan[0], s);
     if (!grp[1].empty()) run_group(grp[1], H.pc_plan[1], split ? H.side : s);
-    if (split) {
-      TABI_CUDA(cudaEventRecord(H.ev_join, H.side));
-      TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
-    }
+    join(split);
     if (any_big) {
+      H.pc_big.alloc(big_leaves.size());
+      TABI_CUDA(cudaMemcpyAsync(H.pc_big.p, big_leaves.data(), sizeof(int) * big_leaves.size(),
+                                cudaMemcpyHostToDevice, s));
       TABI_K(K_LU, s);
-      lu_kernel<<<nl, kLuThreads, 0, s>>>(T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p,
-                                          d_info.p, kPanelMaxM);
+      lu_kernel<<<(int)big_leaves.size(), kLuThreads, 0, s>>>(
+          H.pc_big.p, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, T.d_piv.p, d_info.p, kPanelMaxM);
     }
-  }
   // pivot permutations and inverse diagonal blocks for the applies
   {
     T.dinv_off.resize(nl);
@@ -1496,6 +2070,7 @@ void build_precond(Handle& H, cudaStream_t s) {
     { TABI_K(K_LU_POST, s); lu_diaginv_kernel<<<(int)(dblocks.size() / 4), 128, 0, s>>>(
         H.pc_dblocks.p, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_lu.p, T.d_dinv.p,
         d_info.p); }
+  }
   }
   {
     std::vector<int> info(nl);
@@ -1560,7 +2135,13 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
     TABI_CUDA(cudaEventRecord(H.ev_fork, s));
     TABI_CUDA(cudaStreamWaitEvent(s2, H.ev_fork, 0));
   }
-  if (nbig > 0) {
+  if (nbig > 0 && 2 * T.max_leaf <= kSC * kSCT) {
+    // blocks of order 513..1024: a cluster of kSC CTAs per block
+    TABI_K(K_SOLVE, s);
+    solve_cluster_kernel<<<nbig * kSC, kSCT, 0, s>>>(T.d_leaf_rng.p, T.d_blk_off.p,
+                                                     T.d_dinv_off.p, list, T.d_lu.p, T.d_dinv.p,
+                                                     T.d_lu_perm.p, n, r, z);
+  } else if (nbig > 0) {
     TABI_K(K_SOLVE, s);
     solve_kernel<512><<<nbig, 512, smem, s>>>(T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p,
                                               list, T.d_lu.p, T.d_dinv.p, T.d_lu_perm.p, n, r,

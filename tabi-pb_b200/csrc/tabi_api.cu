@@ -146,6 +146,7 @@ void check_params(const tabi_params& p) {
   TABI_REQUIRE(p.precision == TABI_PREC_FP64 || p.precision == TABI_PREC_MIXED, TABI_ERR_ARG,
                "precision must be TABI_PREC_FP64 or TABI_PREC_MIXED");
   TABI_REQUIRE(p.maxparnode <= 12000, TABI_ERR_LIMIT, "maxparnode above 12000");
+  TABI_REQUIRE((p.flags & ~TABI_FLAG_PIVOTED_LU) == 0, TABI_ERR_ARG, "unknown flags");
 }
 
 void require_tree(Handle& H, int n2) {
@@ -641,6 +642,17 @@ int tabi_counts(tabi_h h, int64_t* near_pairs, int64_t* far_interactions) {
     TABI_REQUIRE(H.has_tree, TABI_ERR_STATE, "no tree");
     if (near_pairs) *near_pairs = H.tree.n_near_pairs;
     if (far_interactions) *far_interactions = H.tree.n_far;
+  });
+}
+
+int tabi_pivoted_leaves(tabi_h h, int* count) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(H.has_precond && H.prm.iprcd == 1, TABI_ERR_STATE,
+                 "no leaf-block preconditioner built");
+    TABI_REQUIRE(count != nullptr, TABI_ERR_ARG, "null argument");
+    *count = H.pc_pv_leaves;
   });
 }
 

@@ -305,6 +305,17 @@ struct Handle {
     DBuf<int> list, mleaves, map;
     DBuf<int4> items, gitems, ritems;
   } pc_plan[2];
+  // the unpivoted factorisation: per group, the diagonal kernels' leaves per
+  // step, panel and update items, and the inverses of the step's diagonal
+  // blocks; per leaf a failed-certificate flag
+  struct NpPlan {
+    DBuf<int> dleaves;
+    DBuf<int4> pitems, gitems;
+    DBuf<double> scr;
+  } pc_np[2];
+  DBuf<int> pc_fail, pc_big;
+  DBuf<int2> pc_tiles2;
+  int pc_pv_leaves = 0;  // leaves of the last tree factored with pivoting
   DBuf<int2> pc_dblocks;
   // staging of the host-array entry points and of tabi_run_dev
   DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;

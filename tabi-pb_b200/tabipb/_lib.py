@@ -34,12 +34,13 @@ SYMBOLS = [
     "tabi_ws_set_params", "tabi_ws_predict_dev", "tabi_ws_loss_grad_dev",
     "tabi_ws_train_step_dev", "tabi_ws_graph_dev", "tabi_set_warmstart", "tabi_batch_run_dev",
     "tabi_output_potential", "tabi_output_potential_dev", "tabi_set_target_range",
-    "tabi_direct_targets",
+    "tabi_direct_targets", "tabi_pivoted_leaves",
 ]
 
 
 PREC_FP64 = 0   # TABI_PREC_FP64: the reference's FP64 arithmetic
 PREC_MIXED = 1  # TABI_PREC_MIXED: FP32 treecode operator, FP64 refinement
+FLAG_PIVOTED_LU = 1  # TABI_FLAG_PIVOTED_LU: partial pivoting for every leaf block
 
 
 class TabiError(RuntimeError):
@@ -128,6 +129,7 @@ def load(path: str = LIB_PATH):
     L.tabi_set_warmstart.argtypes = [_vp, _vp]
     L.tabi_set_target_range.argtypes = [_vp, C.c_int, C.c_int]
     L.tabi_direct_targets.argtypes = [_vp, C.c_int, _ip, _dp, _dp]
+    L.tabi_pivoted_leaves.argtypes = [_vp, _ip]
     L.tabi_output_potential.argtypes = [_vp, C.c_int, _dp, C.c_int, _ip, _dp, _dp, _dp]
     L.tabi_output_potential_dev.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp, _vp, _vp, _vp, _vp]
     L.tabi_batch_run_dev.argtypes = [C.POINTER(Params), C.c_int, C.POINTER(MolDev), _vp, C.c_int,

@@ -227,6 +227,12 @@ class TabiSolver:
                                                    iptr(nv), dptr(x), dptr(xo), dptr(vert)))
         return xo, vert
 
+    def pivoted_leaves(self):
+        """Leaf blocks factored with partial pivoting (tabi_pivoted_leaves)."""
+        c = C.c_int()
+        check(self.h, self.L.tabi_pivoted_leaves(self.h, C.byref(c)))
+        return c.value
+
     def counts(self):
         a, b = C.c_int64(), C.c_int64()
         check(self.h, self.L.tabi_counts(self.h, C.byref(a), C.byref(b)))

@@ -1,4 +1,6 @@
-"""The leaf-block LU's three panel paths, chosen by the rows a panel has left
+"""The leaf-block LU's paths on single large blocks: the certified
+unpivoted factorisation (the default), and, with TABI_FLAG_PIVOTED_LU, the
+pivoted kernels' three panel paths, chosen by the rows a panel has left
 (block order m = 2 x leaf faces): the register-resident panel for up to 1,024
 rows, the shared-memory panel above that (blocks up to 1,536), and the
 global-memory LU for larger blocks.  Each case is one leaf, so one
@@ -22,8 +24,9 @@ CASES = {
 }
 
 
+@pytest.mark.parametrize("flags", [0, 1])
 @pytest.mark.parametrize("name", list(CASES))
-def test_msolve_one_large_block(name, gpu_lib):
+def test_msolve_one_large_block(name, flags, gpu_lib):
     import oracle as O
     import tabipb
 
@@ -31,12 +34,13 @@ def test_msolve_one_large_block(name, gpu_lib):
     case = mk()
     kap = O.kappa(BULK, EPS1)
     with tabipb.TabiSolver(order=3, maxparnode=leaf, theta=0.8, kappa=kap, eps0=EPS0,
-                           eps1=EPS1, iprcd=1) as s:
+                           eps1=EPS1, iprcd=1, flags=flags) as s:
         s.form_matrix(case["sptpos"], case["sptnrm"], case["nvert"], case["chrpos"],
                       case["atmchr"])
         s.build_tree()
         _, sizes = s.leaves()
         assert sizes.size == 1 and 2 * int(sizes[0]) == m
+        assert s.pivoted_leaves() == flags
         oxyz, otq, oar, ob = O.form_matrix(case["sptpos"], case["sptnrm"], case["nvert"],
                                            case["chrpos"], case["atmchr"], EPS0)
         T = O.Tree(oxyz, otq, oar, ob, 3, leaf, 0.8)

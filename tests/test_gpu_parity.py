@@ -16,13 +16,13 @@ MATVEC_TOL = 1e-10
 ENERGY_TOL = 1e-8
 
 
-def _setup(case, order=3, maxparnode=500, theta=0.8, iprcd=1):
+def _setup(case, order=3, maxparnode=500, theta=0.8, iprcd=1, flags=0):
     import oracle as O
     import tabipb
 
     kap = O.kappa(BULK, EPS1)
     s = tabipb.TabiSolver(order=order, maxparnode=maxparnode, theta=theta, kappa=kap,
-                          eps0=EPS0, eps1=EPS1, iprcd=iprcd)
+                          eps0=EPS0, eps1=EPS1, iprcd=iprcd, flags=flags)
     xyz, tq, ar, b = s.form_matrix(case["sptpos"], case["sptnrm"], case["nvert"],
                                    case["chrpos"], case["atmchr"])
     oxyz, otq, oar, ob = O.form_matrix(case["sptpos"], case["sptnrm"], case["nvert"],
@@ -58,7 +58,17 @@ CASES = {
     # MSOLVEprec (main.f90:532-542): diagonal scaling instead of the leaf blocks
     "mol60_L200_iprcd0": (lambda: molecule_case(60, 6.0, 2.0, seed=1), dict(maxparnode=200,
                                                                              iprcd=0)),
+    # two of its 75 leaf blocks need row interchanges (DGETRF2 swaps 4 rows):
+    # they fail the no-interchange check and are factored with pivoting
+    "mol60_d3_L100": (lambda: molecule_case(60, 6.0, 3.0, seed=3), dict(maxparnode=100)),
+    # every leaf with partial pivoting (TABI_FLAG_PIVOTED_LU)
+    "mol60_L200_pivoted": (lambda: molecule_case(60, 6.0, 2.0, seed=1), dict(maxparnode=200,
+                                                                              flags=1)),
 }
+
+# leaf blocks that need partial pivoting, per case (the others take the
+# certified unpivoted factorisation)
+PIVOTED = {"mol60_d3_L100": 2, "mol60_L200_pivoted": 54}
 
 
 @pytest.fixture(scope="module", params=list(CASES))
@@ -137,6 +147,13 @@ def test_matvec_zero_shortcut(setup):
     x = np.zeros(2 * s.nface)
     x[3] = 1e-12  # sum|x| < 1e-10: MATVECmain returns y = x
     assert np.array_equal(s.matvec(x), x)
+
+
+def test_pivoted_leaves(setup):
+    name, case, s, T, kap, g, o = setup
+    if T.iprcd != 1:
+        return
+    assert s.pivoted_leaves() == PIVOTED.get(name, 0)
 
 
 def test_msolve(setup):
