@@ -14,8 +14,6 @@
 // never changes, so here it is assembled and factored once per tree
 // (right-looking LU with partial pivoting, the same pivot rule, batched over
 // all leaves) and every apply is a blocked forward/back substitution.
-#include <cooperative_groups.h>
-
 #include <algorithm>
 #include <climits>
 
@@ -1268,10 +1266,26 @@ constexpr size_t kNPPanelSmem = sizeof(double) * 2 * kNP * kNPPitch;
 
 // Per leaf (leaves[blockIdx.x]) with m > k0: D = A[k0:k0+d, k0:k0+d], d =
 // min(64, m - k0), factored in place without interchanges (DGETRF2's scaling:
-// reciprocal unless the pivot is below the smallest normal); scr receives
-// L^{-1} (unit lower) and U^{-1} of D (64 x 64 each, column-major, zeros
-// outside the triangle), dinv the 32 x 32 diagonal blocks of both (identity
-// padded), the layout lu_diaginv_kernel writes.
+// reciprocal unless the pivot is below the smallest normal; the rank-1 updates
+// on a 16 x 16 thread grid); scr receives L^{-1} (unit lower, column-major)
+// and U^{-1} (row-major) of D, 64 x 64 each with zeros outside the triangle,
+// and dinv the 32 x 32 diagonal blocks of both (identity padded, the layout
+// lu_diaginv_kernel writes).  The inverses go by 32 x 32 blocks: four warps
+// invert the diagonal blocks of L and U (one column per lane, unrolled), then
+// L^{-1}_21 = -L22^{-1} (L21 L11^{-1}) and U^{-1}_12 = -U11^{-1} (U12 U22^{-1})
+// by two small products through the zero blocks of the result as scratch.
+// one double into shared memory, asynchronously (zero when !valid)
+__device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+               "r"(valid ? 8 : 0));
+}
+
+__device__ __forceinline__ double np_entry(const double (*D)[kNPPitch], int o, int nb, int i,
+                                           int q) {
+  return (i < nb && q < nb) ? D[o + i][o + q] : (i == q ? 1.0 : 0.0);
+}
+
 __global__ void __launch_bounds__(kNPT) lu_np_diag_kernel(
     const int* __restrict__ leaves, int k0, const int2* __restrict__ leaf_rng,
     const int64_t* __restrict__ blk_off, const int64_t* __restrict__ dinv_off,
@@ -1285,72 +1299,224 @@ __global__ void __launch_bounds__(kNPT) lu_np_diag_kernel(
   const int m = 2 * leaf_rng[leaf].y;
   const int d = min(kNP, m - k0);
   double* A = lu + blk_off[leaf];
-  const int tid = threadIdx.x;
-  for (int e = tid; e < d * d; e += kNPT) {
-    const int c = e / d, r = e - c * d;
-    D[r][c] = A[(size_t)(k0 + c) * m + k0 + r];
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int e = tid; e < kNP * kNP; e += kNPT) {
+    const int c = e >> 6, r = e & 63;
+    cp_async8(&D[r][c], A + (size_t)(k0 + min(c, d - 1)) * m + k0 + min(r, d - 1),
+              r < d && c < d);
   }
+  asm volatile("cp.async.commit_group;\n" ::);
+  for (int e = tid; e < kNP * kNPPitch; e += kNPT) {
+    (&Li[0][0])[e] = 0.0;
+    (&Ui[0][0])[e] = 0.0;
+  }
+  __shared__ double s_rcp[kNP];  // reciprocal of each pivot
+  asm volatile("cp.async.wait_group 0;\n" ::);
   __syncthreads();
+  // 2 x 2 blocks of 32: LU(D11) by warp 0 in registers; U12 = L11^{-1} D12
+  // (warp 1) and L21 = D21 U11^{-1} (warp 2); D22 -= L21 U12 (all warps);
+  // LU(D22) by warp 0.  DGETRF2's scaling throughout: a multiplier is the
+  // updated entry times the pivot's reciprocal (divided when the pivot is
+  // below the smallest normal).
   bool bad = false;
-  for (int j = 0; j < d; ++j) {
-    const double pk = D[j][j];
-    if (!(pk != 0.0 && isfinite(pk))) bad = true;
-    const bool recip = fabs(pk) >= 2.2250738585072014e-308;
-    const double rcp = 1.0 / pk;
-    if (tid > j && tid < d) {
-      const double l = recip ? D[tid][j] * rcp : D[tid][j] / pk;
-      if (!(fabs(l) <= kNoPivBound)) bad = true;
-      D[tid][j] = l;
+  const int n2 = max(0, d - kDB);
+  for (int blk = 0; blk < 2; ++blk) {
+    const int o = blk * kDB, nb = blk == 0 ? min(kDB, d) : n2;
+    if (nb > 0 && warp == 0) {
+      const int r = lane;  // this lane's row of the block
+      double a[kDB];
+#pragma unroll
+      for (int c = 0; c < kDB; ++c) a[c] = (r < nb && c < nb) ? D[o + r][o + c] : 0.0;
+#pragma unroll
+      for (int j = 0; j < kDB; ++j) {
+        if (j < nb) {
+          const double pk = __shfl_sync(0xffffffffu, a[j], j);
+          if (!(pk != 0.0 && isfinite(pk))) bad = true;
+          const bool recip = fabs(pk) >= 2.2250738585072014e-308;
+          const double rcp = 1.0 / pk;
+          if (lane == 0) s_rcp[o + j] = recip ? rcp : 0.0;
+          const double l = recip ? a[j] * rcp : a[j] / pk;
+          if (r > j && r < nb) {
+            if (!(fabs(l) <= kNoPivBound)) bad = true;
+            a[j] = l;
+          }
+#pragma unroll
+          for (int c = j + 1; c < kDB; ++c) {
+            const double u = __shfl_sync(0xffffffffu, a[c], j);
+            if (r > j && r < nb) a[c] = fma(-l, u, a[c]);
+          }
+        }
+      }
+      if (r < nb)
+#pragma unroll
+        for (int c = 0; c < kDB; ++c)
+          if (c < nb) D[o + r][o + c] = a[c];
     }
     __syncthreads();
-    const int w = d - 1 - j;
-    for (int e = tid; e < w * w; e += kNPT) {
-      const int i = j + 1 + e % w, c = j + 1 + e / w;
-      D[i][c] = fma(-D[i][j], D[j][c], D[i][c]);
+    if (blk == 1 || n2 == 0) break;
+    if (warp == 1 && lane < n2) {
+      // U12: column kDB + lane of the block row, forward substitution with L11
+      const int c = kDB + lane;
+      double x[kDB];
+#pragma unroll
+      for (int r = 0; r < kDB; ++r) {
+        double v = D[r][c];
+#pragma unroll
+        for (int q = 0; q < kDB; ++q)
+          if (q < r) v = fma(-D[r][q], x[q], v);
+        x[r] = v;
+      }
+#pragma unroll
+      for (int r = 0; r < kDB; ++r) D[r][c] = x[r];
+    } else if (warp == 2 && lane < n2) {
+      // L21: row kDB + lane, x U11 = D21 row, with the pivots' reciprocals
+      const int r = kDB + lane;
+      double x[kDB];
+#pragma unroll
+      for (int c = 0; c < kDB; ++c) {
+        double v = D[r][c];
+#pragma unroll
+        for (int q = 0; q < kDB; ++q)
+          if (q < c) v = fma(-x[q], D[q][c], v);
+        const double pk = D[c][c], rc = s_rcp[c];
+        v = rc != 0.0 ? v * rc : v / pk;
+        if (!(fabs(v) <= kNoPivBound)) bad = true;
+        x[c] = v;
+      }
+#pragma unroll
+      for (int c = 0; c < kDB; ++c) D[r][c] = x[c];
+    }
+    __syncthreads();
+    // D22 -= L21 U12: thread (row tid / 8, columns 4 (tid % 8) ..)
+    {
+      const int r = tid >> 3, c4 = (tid & 7) * 4;
+      if (r < n2) {
+        double acc[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[b] = D[kDB + r][kDB + c4 + b];
+#pragma unroll 8
+        for (int q = 0; q < kDB; ++q) {
+          const double l = D[kDB + r][q];
+#pragma unroll
+          for (int b = 0; b < 4; ++b) acc[b] = fma(-l, D[q][kDB + c4 + b], acc[b]);
+        }
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+          if (c4 + b < n2) D[kDB + r][kDB + c4 + b] = acc[b];
+      }
     }
     __syncthreads();
   }
-  // inverses, one column per thread: threads 0..d-1 L^{-1}, 64..64+d-1 U^{-1}
-  if (tid < d) {
-    const int c = tid;
-    for (int i = 0; i < kNP; ++i) Li[i][c] = 0.0;
-    Li[c][c] = 1.0;
-    for (int i = c + 1; i < d; ++i) {
-      double v0 = 0.0, v1 = 0.0;
-      int q = c;
-      for (; q + 1 < i; q += 2) {
-        v0 = fma(-D[i][q], Li[q][c], v0);
-        v1 = fma(-D[i][q + 1], Li[q + 1][c], v1);
-      }
-      if (q < i) v0 = fma(-D[i][q], Li[q][c], v0);
-      Li[i][c] = v0 + v1;
-    }
-  } else if (tid >= kNP && tid < kNP + d) {
-    const int c = tid - kNP;
-    for (int i = 0; i < kNP; ++i) Ui[i][c] = 0.0;
-    Ui[c][c] = 1.0 / D[c][c];
-    for (int i = c - 1; i >= 0; --i) {
-      double v0 = 0.0, v1 = 0.0;
-      int q = i + 1;
-      for (; q + 1 <= c; q += 2) {
-        v0 = fma(-D[i][q], Ui[q][c], v0);
-        v1 = fma(-D[i][q + 1], Ui[q + 1][c], v1);
-      }
-      if (q <= c) v0 = fma(-D[i][q], Ui[q][c], v0);
-      Ui[i][c] = (v0 + v1) / D[i][i];
-    }
-  }
-  if (__syncthreads_or(bad) && tid == 0) fail[leaf] = 1;
-  // factors back, inverses out
+  // factors back
   for (int e = tid; e < d * d; e += kNPT) {
     const int c = e / d, r = e - c * d;
     A[(size_t)(k0 + c) * m + k0 + r] = D[r][c];
   }
+  // inverses of the 32 x 32 diagonal blocks: warp 0/1 L (blocks 0/1), warp 2/3 U
+  if (warp < 4) {
+    const int b = warp & 1, o = b * kDB, nb = min(kDB, d - o);
+    if (nb > 0) {
+      double x[kDB];
+      if (warp < 2) {
+#pragma unroll
+        for (int i = 0; i < kDB; ++i) {
+          double v = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+          for (int q = 0; q < kDB; ++q)
+            if (q < i) v = fma(-np_entry(D, o, nb, i, q), x[q], v);
+          x[i] = v;
+        }
+        if (lane < nb)
+#pragma unroll
+          for (int i = 0; i < kDB; ++i)
+            if (i < nb) Li[o + i][o + lane] = x[i];
+      } else {
+#pragma unroll
+        for (int i = kDB - 1; i >= 0; --i) {
+          double v = (i == lane) ? 1.0 : 0.0;
+#pragma unroll
+          for (int q = 0; q < kDB; ++q)
+            if (q > i) v = fma(-np_entry(D, o, nb, i, q), x[q], v);
+          x[i] = v / np_entry(D, o, nb, i, i);
+        }
+        if (lane < nb)
+#pragma unroll
+          for (int i = 0; i < kDB; ++i)
+            if (i < nb) Ui[o + i][o + lane] = x[i];
+      }
+    }
+  }
+  __syncthreads();
+  if (d > kDB) {
+    const int n2 = d - kDB;  // order of the second diagonal block
+    // T = L21 L11^{-1} into Li's (zero) upper-right block, T' = U12 U22^{-1}
+    // into Ui's (zero) lower-left block
+    for (int e = tid; e < kDB * kDB; e += kNPT) {
+      const int r = e / kDB, c = e - r * kDB;
+      // full 32-term sums (the inverses are zero outside their triangles),
+      // two accumulators each
+      if (r < n2) {  // T[r][c], r < n2, c < 32
+        double v0 = 0.0, v1 = 0.0;
+#pragma unroll
+        for (int q = 0; q < kDB; q += 2) {
+          v0 = fma(D[kDB + r][q], Li[q][c], v0);
+          v1 = fma(D[kDB + r][q + 1], Li[q + 1][c], v1);
+        }
+        Li[c][kDB + r] = v0 + v1;  // stored transposed in the free block
+      }
+      if (c < n2) {  // T'[r][c], r < 32, c < n2
+        double v0 = 0.0, v1 = 0.0;
+#pragma unroll
+        for (int q = 0; q < kDB; q += 2) {
+          v0 = fma(D[r][kDB + q], Ui[kDB + q][kDB + c], v0);
+          v1 = fma(D[r][kDB + q + 1], Ui[kDB + q + 1][kDB + c], v1);
+        }
+        Ui[kDB + c][r] = v0 + v1;  // transposed
+      }
+    }
+    __syncthreads();
+    double l21[4], u12[4];
+    int nv = 0;
+    for (int e = tid; e < kDB * kDB; e += kNPT, ++nv) {
+      const int r = e / kDB, c = e - r * kDB;
+      double a = 0.0, bb = 0.0;
+      if (r < n2) {  // -(L22^{-1} T)[r][c]
+        double a1 = 0.0;
+#pragma unroll
+        for (int q = 0; q < kDB; q += 2) {
+          a = fma(Li[kDB + r][kDB + q], Li[c][kDB + q], a);
+          a1 = fma(Li[kDB + r][kDB + q + 1], Li[c][kDB + q + 1], a1);
+        }
+        a += a1;
+      }
+      if (c < n2) {  // -(U11^{-1} T')[r][c]
+        double b1 = 0.0;
+#pragma unroll
+        for (int q = 0; q < kDB; q += 2) {
+          bb = fma(Ui[r][q], Ui[kDB + c][q], bb);
+          b1 = fma(Ui[r][q + 1], Ui[kDB + c][q + 1], b1);
+        }
+        bb += b1;
+      }
+      l21[nv] = -a;
+      u12[nv] = -bb;
+    }
+    __syncthreads();
+    nv = 0;
+    for (int e = tid; e < kDB * kDB; e += kNPT, ++nv) {
+      const int r = e / kDB, c = e - r * kDB;
+      Li[c][kDB + r] = 0.0;
+      Ui[kDB + c][r] = 0.0;
+      if (r < n2) Li[kDB + r][c] = l21[nv];
+      if (c < n2) Ui[r][kDB + c] = u12[nv];
+    }
+  }
+  if (__syncthreads_or(bad) && tid == 0) fail[leaf] = 1;
   double* S = scr + (size_t)blockIdx.x * 2 * kNP * kNP;
   for (int e = tid; e < kNP * kNP; e += kNPT) {
-    const int c = e / kNP, r = e - c * kNP;
-    S[e] = (r < d && c < d) ? Li[r][c] : 0.0;
-    S[kNP * kNP + e] = (r < d && c < d) ? Ui[r][c] : 0.0;
+    const int hi = e / kNP, lo = e - hi * kNP;
+    S[e] = Li[lo][hi];            // column-major L^{-1}
+    S[kNP * kNP + e] = Ui[hi][lo];  // row-major U^{-1}
   }
   double* Di = dinv + dinv_off[leaf] + (size_t)(k0 / kDB) * 2 * kDB * kDB;
   for (int b = 0; b * kDB < d; ++b) {
@@ -1369,7 +1535,9 @@ __global__ void __launch_bounds__(kNPT) lu_np_diag_kernel(
 // item = (leaf, slot, kind, off): kind 0, rows [off, off + 64) of the step's
 // column panel: L21 = A21 U11^{-1}, each multiplier checked; kind 1, columns
 // [off, off + 64) of its row panel: U12 = L11^{-1} A12.  slot = the leaf's
-// row in the diagonal kernel's launch (its scratch).
+// row in the diagonal kernel's launch (its scratch).  A 64 x 64 x 64 product
+// out = P Q from shared memory, 4 x 4 outputs per thread (rows tr + 16 a,
+// columns tc + 16 b: P loads on 16 consecutive rows, Q loads broadcast).
 __global__ void __launch_bounds__(kNPT) lu_np_panel_kernel(
     const int4* __restrict__ items, int k0, const int2* __restrict__ leaf_rng,
     const int64_t* __restrict__ blk_off, double* __restrict__ lu,
@@ -1384,90 +1552,99 @@ __global__ void __launch_bounds__(kNPT) lu_np_panel_kernel(
   const int cnt = min(kNP, m - off);
   double* A = lu + blk_off[leaf];
   const double* S = scr + (size_t)it.y * 2 * kNP * kNP + (kind == 0 ? kNP * kNP : 0);
-  const int tid = threadIdx.x;
-  // V[a][b] = the inverse (L^{-1} or U^{-1}), zeros outside d x d
+  const int tid = threadIdx.x, tr = tid & 15, tc = tid >> 4;
+  // V = the inverse as [row][col]: U^{-1} (row-major in scr) for kind 0,
+  // L^{-1} (column-major in scr) for kind 1; zeros outside d x d
   for (int e = tid; e < kNP * kNP; e += kNPT) {
-    const int c = e / kNP, r = e - c * kNP;
-    V[r][c] = S[e];
+    const int hi = e >> 6, lo = e & 63;
+    cp_async8(kind == 0 ? &V[hi][lo] : &V[lo][hi], S + e, true);
+  }
+  if (kind == 0) {  // X[i][q] = A[off + i, k0 + q]
+    for (int e = tid; e < kNP * kNP; e += kNPT) {
+      const int q = e >> 6, i = e & 63;
+      const bool ok = i < cnt && q < d;
+      cp_async8(&X[i][q], ok ? A + (size_t)(k0 + q) * m + off + i : A, ok);
+    }
+  } else {          // X[q][c] = A[k0 + q, off + c]
+    for (int e = tid; e < kNP * kNP; e += kNPT) {
+      const int c = e >> 6, q = e & 63;
+      const bool ok = c < cnt && q < d;
+      cp_async8(&X[q][c], ok ? A + (size_t)(off + c) * m + k0 + q : A, ok);
+    }
+  }
+  asm volatile("cp.async.commit_group;\n" ::);
+  asm volatile("cp.async.wait_group 0;\n" ::);
+  __syncthreads();
+  // kind 0: out = X V (P = X, Q = V); kind 1: out = V X (P = V, Q = X)
+  const double(*P)[kNPPitch] = kind == 0 ? X : V;
+  const double(*Q)[kNPPitch] = kind == 0 ? V : X;
+  double acc[4][4];
+#pragma unroll
+  for (int a = 0; a < 4; ++a)
+#pragma unroll
+    for (int b = 0; b < 4; ++b) acc[a][b] = 0.0;
+#pragma unroll 4
+  for (int q = 0; q < d; ++q) {
+    double pv[4], qv[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) pv[a] = P[tr + 16 * a][q];
+#pragma unroll
+    for (int b = 0; b < 4; ++b) qv[b] = Q[q][tc + 16 * b];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+      for (int b = 0; b < 4; ++b) acc[a][b] = fma(pv[a], qv[b], acc[a][b]);
   }
   bool bad = false;
-  if (kind == 0) {
-    // X[i][q] = A[off + i, k0 + q]
-    for (int e = tid; e < kNP * kNP; e += kNPT) {
-      const int q = e / kNP, i = e - q * kNP;
-      X[i][q] = (i < cnt && q < d) ? A[(size_t)(k0 + q) * m + off + i] : 0.0;
-    }
-    __syncthreads();
-    const int i = tid % kNP, c0 = (tid / kNP) * 16;
-    double acc[16];
 #pragma unroll
-    for (int cc = 0; cc < 16; ++cc) acc[cc] = 0.0;
-    for (int q = 0; q < d; ++q) {
-      const double x = X[i][q];
+  for (int a = 0; a < 4; ++a)
 #pragma unroll
-      for (int cc = 0; cc < 16; ++cc) acc[cc] = fma(x, V[q][c0 + cc], acc[cc]);
-    }
-    if (i < cnt) {
-#pragma unroll
-      for (int cc = 0; cc < 16; ++cc) {
-        const int c = c0 + cc;
-        if (c < d) {
-          if (!(fabs(acc[cc]) <= kNoPivBound)) bad = true;
-          A[(size_t)(k0 + c) * m + off + i] = acc[cc];
+    for (int b = 0; b < 4; ++b) {
+      const int r = tr + 16 * a, c = tc + 16 * b;
+      if (kind == 0) {
+        if (r < cnt && c < d) {
+          if (!(fabs(acc[a][b]) <= kNoPivBound)) bad = true;
+          A[(size_t)(k0 + c) * m + off + r] = acc[a][b];
         }
+      } else if (c < cnt && r < d) {
+        A[(size_t)(off + c) * m + k0 + r] = acc[a][b];
       }
     }
-  } else {
-    // X[q][c] = A[k0 + q, off + c]
-    for (int e = tid; e < kNP * kNP; e += kNPT) {
-      const int c = e / kNP, q = e - c * kNP;
-      X[q][c] = (c < cnt && q < d) ? A[(size_t)(off + c) * m + k0 + q] : 0.0;
-    }
-    __syncthreads();
-    const int c = tid % kNP, r0 = (tid / kNP) * 16;
-    double acc[16];
-#pragma unroll
-    for (int rr = 0; rr < 16; ++rr) acc[rr] = 0.0;
-    for (int q = 0; q < d; ++q) {
-      const double x = X[q][c];
-#pragma unroll
-      for (int rr = 0; rr < 16; ++rr) acc[rr] = fma(V[r0 + rr][q], x, acc[rr]);
-    }
-    if (c < cnt) {
-#pragma unroll
-      for (int rr = 0; rr < 16; ++rr)
-        if (r0 + rr < d) A[(size_t)(off + c) * m + k0 + r0 + rr] = acc[rr];
-    }
-  }
   if (__syncthreads_or(bad) && tid == 0) fail[leaf] = 1;
 }
 
-// Trailing update of the unpivoted factorisation: item = (leaf, r0, c0, 0):
+// Updates of the unpivoted factorisation: item = (leaf, r0, c0, ends):
 // C = A[r0:r0+128, c0:c0+64] -= A[r0:, k0:k0+kd] A[k0:k0+kd, c0:] with
-// kd = min(64, m - k0), rows and columns clipped at m.  256 threads, 8 x 4
+// kd = min(kdepth, m - k0) (64 inside an outer block of kOB2 columns, kOB2
+// for the trailing matrix right of it), rows clipped at re and columns at ce,
+// packed as ends = (re << 16) | ce (0: both m).  256 threads, 8 x 4
 // outputs each: rows 2 tr + 32 a + {0, 1} (a = 0..3; each pair one 16-byte
 // shared load, eight lanes of a load phase on 32 distinct banks) and columns
 // 4 tc .. 4 tc + 3 (two 16-byte loads, broadcast within a phase).  C is loaded
 // into the accumulators and the products subtracted one k at a time
 // (fma(-l, u, c)), the order of the reference's DGEMM (C := C - A B,
-// dgetrf_dep.f), while the two 32-deep slices of L and U arrive by cp.async
+// dgetrf_dep.f), while the 32-deep slices of L (k-major) and U (by column,
+// pitch 34: conflict-free 16-byte stores, broadcast loads) arrive by cp.async
 // (zero-filled outside the tile: m, r0, c0, k0 and the depth are even, so a
-// 16-byte chunk of L is wholly inside or outside; U comes in 8-byte copies,
-// being transposed to k-major).
+// 16-byte chunk is wholly inside or outside).
 constexpr int kG2M = 128, kG2N = 64, kG2K = 32;
-constexpr size_t kGemm2Smem = sizeof(double) * 2 * (kG2K * kG2M + kG2K * kG2N);
+constexpr int kG2UP = kG2K + 2;  // U slice by column: pitch of 34 doubles
+constexpr int kOB2 = 256;  // outer block of the unpivoted factorisation
+constexpr size_t kGemm2Smem = sizeof(double) * 2 * (kG2K * kG2M + kG2N * kG2UP);
 
 __global__ void __launch_bounds__(256, 2) lu_gemm2_kernel(const int4* __restrict__ items, int k0,
+                                                          int kdepth,
                                                           const int2* __restrict__ leaf_rng,
                                                           const int64_t* __restrict__ blk_off,
                                                           double* __restrict__ lu) {
   extern __shared__ double gsm2[];
   double* sL = gsm2;                      // [2][kG2K][kG2M]  L slice, k-major
-  double* sU = gsm2 + 2 * kG2K * kG2M;    // [2][kG2K][kG2N]  U slice, k-major
+  double* sU = gsm2 + 2 * kG2K * kG2M;    // [2][kG2N][kG2UP] U slice, by column
   const int4 it = items[blockIdx.x];
   const int leaf = it.x, r0 = it.y, c0 = it.z;
   const int m = 2 * leaf_rng[leaf].y;
-  const int kd = min(kNP, m - k0);
+  const int re = it.w ? min(m, it.w >> 16) : m, ce = it.w ? min(m, it.w & 0xffff) : m;
+  const int kd = min(kdepth, m - k0);
   double* A = lu + blk_off[leaf];
   const int tid = threadIdx.x;
   const int tr = tid & 15, tc = tid >> 4;
@@ -1475,40 +1652,40 @@ __global__ void __launch_bounds__(256, 2) lu_gemm2_kernel(const int4* __restrict
   auto load_slice = [&](int kc, int buf) {
     const int nbk = min(kG2K, kd - kc), kb = k0 + kc;
     double* L = sL + buf * kG2K * kG2M;
-    double* U = sU + buf * kG2K * kG2N;
+    double* U = sU + buf * kG2N * kG2UP;
 #pragma unroll
     for (int e = 0; e < (kG2K * kG2M / 2) / 256; ++e) {
       const int q = tid + 256 * e;
       const int k = q / (kG2M / 2), rr = 2 * (q % (kG2M / 2));
-      const bool ok = k < nbk && r0 + rr < m;
+      const bool ok = k < nbk && r0 + rr < re;
       cp_async16(L + k * kG2M + rr, ok ? A + (size_t)(kb + k) * m + r0 + rr : A, ok);
     }
+    // U by column (the source's own layout): 16-byte chunks of 2 k
 #pragma unroll
     for (int e = 0; e < (kG2K * kG2N / 2) / 256; ++e) {
       const int q = tid + 256 * e;
       const int c = q / (kG2K / 2), kk = 2 * (q % (kG2K / 2));
-      const bool ok = kk < nbk && c0 + c < m;
-      const double* src = ok ? A + (size_t)(c0 + c) * m + kb + kk : A;
-      const unsigned d0 = (unsigned)__cvta_generic_to_shared(U + kk * kG2N + c);
-      const unsigned d1 = (unsigned)__cvta_generic_to_shared(U + (kk + 1) * kG2N + c);
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d0), "l"(src),
-                   "r"(ok ? 8 : 0));
-      asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d1), "l"(src + 1),
-                   "r"(ok ? 8 : 0));
+      const bool ok = kk < nbk && c0 + c < ce;
+      cp_async16(U + c * kG2UP + kk, ok ? A + (size_t)(c0 + c) * m + kb + kk : A, ok);
     }
     asm volatile("cp.async.commit_group;\n" ::);
   };
   load_slice(0, 0);
   if (kG2K < kd) load_slice(kG2K, 1);
+  // C by row pairs: 16 lanes read 256 contiguous bytes of a column (rows and
+  // m are even, so a pair is wholly inside or outside)
   double acc[8][4];
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
     const int c = c0 + 4 * tc + b;
     const double* cc = A + (size_t)min(c, m - 1) * m;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
+    for (int a = 0; a < 8; a += 2) {
       const int r = r0 + row_of(a);
-      acc[a][b] = (c < m && r < m) ? cc[r] : 0.0;
+      const double2 v = (c < ce && r < re) ? *reinterpret_cast<const double2*>(cc + r)
+                                           : make_double2(0.0, 0.0);
+      acc[a][b] = v.x;
+      acc[a + 1][b] = v.y;
     }
   }
   for (int kc = 0, buf = 0; kc < kd; kc += kG2K, buf ^= 1) {
@@ -1518,34 +1695,54 @@ __global__ void __launch_bounds__(256, 2) lu_gemm2_kernel(const int4* __restrict
       asm volatile("cp.async.wait_group 0;\n" ::);
     }
     __syncthreads();
+    // all 32 k of the slice (zero-filled past the depth: fma(-0, 0, c) = c),
+    // the next k's operands loaded while this k's products run
     const double* L = sL + buf * kG2K * kG2M + 2 * tr;
-    const double* U = sU + buf * kG2K * kG2N + 4 * tc;
-    const int nbk = min(kG2K, kd - kc);
-#pragma unroll 4
-    for (int k = 0; k < nbk; ++k) {
-      const double2 l01 = *reinterpret_cast<const double2*>(L + k * kG2M);
-      const double2 l23 = *reinterpret_cast<const double2*>(L + k * kG2M + 32);
-      const double2 l45 = *reinterpret_cast<const double2*>(L + k * kG2M + 64);
-      const double2 l67 = *reinterpret_cast<const double2*>(L + k * kG2M + 96);
-      const double2 u01 = *reinterpret_cast<const double2*>(U + k * kG2N);
-      const double2 u23 = *reinterpret_cast<const double2*>(U + k * kG2N + 2);
-      const double lv[8] = {l01.x, l01.y, l23.x, l23.y, l45.x, l45.y, l67.x, l67.y};
-      const double uv[4] = {u01.x, u01.y, u23.x, u23.y};
+    const double* U = sU + buf * kG2N * kG2UP + 4 * tc * kG2UP;
+    double2 lc[4];
+    double uc[4];
+#pragma unroll
+    for (int a = 0; a < 4; ++a) lc[a] = *reinterpret_cast<const double2*>(L + 32 * a);
+#pragma unroll
+    for (int b = 0; b < 4; ++b) uc[b] = U[b * kG2UP];
+#pragma unroll
+    for (int k = 0; k < kG2K; ++k) {
+      double2 ln[4];
+      double un[4];
+      if (k + 1 < kG2K) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+          ln[a] = *reinterpret_cast<const double2*>(L + (k + 1) * kG2M + 32 * a);
+#pragma unroll
+        for (int b = 0; b < 4; ++b) un[b] = U[b * kG2UP + k + 1];
+      }
+      const double lv[8] = {lc[0].x, lc[0].y, lc[1].x, lc[1].y,
+                            lc[2].x, lc[2].y, lc[3].x, lc[3].y};
 #pragma unroll
       for (int a = 0; a < 8; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = fma(-lv[a], uv[b], acc[a][b]);
+        for (int b = 0; b < 4; ++b) acc[a][b] = fma(-lv[a], uc[b], acc[a][b]);
+      if (k + 1 < kG2K) {
+#pragma unroll
+        for (int a = 0; a < 4; ++a) lc[a] = ln[a];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) uc[b] = un[b];
+      }
+    }
+    if (kc + 2 * kG2K < kd) {  // buffer buf takes the slice two on
+      __syncthreads();
+      load_slice(kc + 2 * kG2K, buf);
     }
   }
 #pragma unroll
   for (int b = 0; b < 4; ++b) {
     const int c = c0 + 4 * tc + b;
-    if (c >= m) continue;
+    if (c >= ce) continue;
     double* cc = A + (size_t)c * m;
 #pragma unroll
-    for (int a = 0; a < 8; ++a) {
+    for (int a = 0; a < 8; a += 2) {
       const int r = r0 + row_of(a);
-      if (r < m) cc[r] = acc[a][b];
+      if (r < re) *reinterpret_cast<double2*>(cc + r) = make_double2(acc[a][b], acc[a + 1][b]);
     }
   }
 }
@@ -1559,120 +1756,6 @@ __global__ void lu_np_identity_kernel(const int2* __restrict__ leaf_rng, int* __
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     piv[2 * lr.x + i] = i + 1;
     perm[2 * lr.x + i] = i;
-  }
-}
-
-// The apply of a large leaf block (order 512 < m <= 1024) by a cluster of
-// kSC CTAs: the block's 32-row diagonal blocks are split into kSC contiguous
-// runs, one per CTA, and each thread keeps one row of its CTA's run.  Step t
-// of a sweep: the CTA that owns diagonal block t forms y = D_t^{-1} run_t
-// (the inverse staged in its shared memory one step ahead), keeps it, and
-// writes it into every CTA's shared memory (distributed shared memory,
-// double-buffered by step parity); one cluster barrier; every thread then
-// subtracts its row's 32 products with y (the row's 32 factor entries were
-// loaded before the barrier).  Forward sweep L y = P r over the diagonal
-// blocks in order (rows below each step), backward U x = y in reverse order
-// (rows above).  Each SM streams a quarter of the block's factors, instead of
-// one SM all of it.
-constexpr int kSC = 4;      // CTAs per cluster
-constexpr int kSCT = 256;   // threads per CTA (rows per CTA <= 256: m <= 1024)
-
-__global__ void __cluster_dims__(kSC, 1, 1) __launch_bounds__(kSCT) solve_cluster_kernel(
-    const int2* __restrict__ leaf_rng, const int64_t* __restrict__ blk_off,
-    const int64_t* __restrict__ dinv_off, const int* __restrict__ leaf_list,
-    const double* __restrict__ lu, const double* __restrict__ dinv,
-    const int* __restrict__ perm, int N, const double* __restrict__ r,
-    double* __restrict__ z) {
-  namespace cg = cooperative_groups;
-  cg::cluster_group cl = cg::this_cluster();
-  const int rank = (int)cl.block_rank();
-  __shared__ double xs[kSCT];          // forward: running values; backward: results
-  __shared__ double fs[kSCT];          // forward: results; backward: running values
-  __shared__ double ybuf[2][kDB];      // the step's 32 values, by step parity
-  __shared__ __align__(16) double dbuf[2][kDB * kDB];
-  const int leaf = leaf_list[blockIdx.x / kSC];
-  const int2 lr = leaf_rng[leaf];
-  const int n = lr.y, m = 2 * n, ib = lr.x;
-  const int nblk = (m + kDB - 1) / kDB;
-  auto first_block = [&](int c) { return (c * nblk) / kSC; };
-  auto owner = [&](int b) {  // the rank whose run holds diagonal block b
-    int c = 0;
-    while (c + 1 < kSC && first_block(c + 1) <= b) ++c;
-    return c;
-  };
-  const int R0 = kDB * first_block(rank), R1 = min(m, kDB * first_block(rank + 1));
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const int i = R0 + tid;             // this thread's row
-  const bool mine = i < R1;
-  const double* A = lu + blk_off[leaf];
-  const double* Di = dinv + dinv_off[leaf];
-  if (mine) {
-    const int src = perm[2 * ib + i];
-    xs[tid] = src < n ? r[ib + src] : r[N + ib + src - n];
-  }
-  // the inverse diagonal block of sweep step s (L blocks 0..nblk-1, then U
-  // blocks nblk-1..0) into dbuf[s & 1], by its owner
-  auto block_of = [&](int st) { return st < nblk ? st : 2 * nblk - 1 - st; };
-  auto stage = [&](int st) {
-    if (st >= 2 * nblk || owner(block_of(st)) != rank) return;
-    const int b = block_of(st);
-    const double* src = Di + (size_t)b * 2 * kDB * kDB + (st < nblk ? 0 : kDB * kDB);
-    for (int e = 2 * tid; e < kDB * kDB; e += 2 * kSCT) {
-      const unsigned d = (unsigned)__cvta_generic_to_shared(&dbuf[st & 1][e]);
-      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(src + e));
-    }
-    asm volatile("cp.async.commit_group;\n" ::);
-  };
-  stage(0);
-  asm volatile("cp.async.wait_group 0;\n" ::);
-  __syncthreads();
-  for (int st = 0; st < 2 * nblk; ++st) {
-    const bool fwd = st < nblk;
-    const int b = block_of(st), k0 = b * kDB, nb = min(kDB, m - k0);
-    double* run = fwd ? xs : fs;   // running values of this sweep
-    double* res = fwd ? fs : xs;   // its results
-    // this row's factor entries of the step: L below the block (forward),
-    // U above it (backward)
-    const bool upd = mine && (fwd ? i >= k0 + nb : i < k0);
-    double av[kDB];
-#pragma unroll
-    for (int q = 0; q < kDB; ++q)
-      av[q] = (upd && q < nb) ? A[(size_t)(k0 + q) * m + i] : 0.0;
-    stage(st + 1);
-    if (owner(b) == rank && warp == 0) {
-      const double* D = dbuf[st & 1];
-      double v0 = 0.0, v1 = 0.0;
-      for (int q = 0; q < nb; q += 2) {
-        v0 = fma(D[q * kDB + lane], run[k0 - R0 + q], v0);
-        if (q + 1 < nb) v1 = fma(D[(q + 1) * kDB + lane], run[k0 - R0 + q + 1], v1);
-      }
-      const double y = lane < nb ? v0 + v1 : 0.0;
-      if (lane < nb) res[k0 - R0 + lane] = y;
-#pragma unroll
-      for (int c = 0; c < kSC; ++c) {
-        double* yb = cl.map_shared_rank(&ybuf[st & 1][0], c);
-        yb[lane] = y;
-      }
-    }
-    cl.sync();  // y of this step everywhere (release / acquire)
-    if (upd) {
-      const double* y = ybuf[st & 1];
-      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
-#pragma unroll
-      for (int q = 0; q < kDB; q += 4) {
-        s0 = fma(av[q], y[q], s0);
-        s1 = fma(av[q + 1], y[q + 1], s1);
-        s2 = fma(av[q + 2], y[q + 2], s2);
-        s3 = fma(av[q + 3], y[q + 3], s3);
-      }
-      run[tid] -= (s0 + s1) + (s2 + s3);
-    }
-    asm volatile("cp.async.wait_group 0;\n" ::);
-    __syncthreads();
-  }
-  if (mine) {
-    if (i < n) z[ib + i] = xs[tid];
-    else z[N + ib + i - n] = xs[tid];
   }
 }
 
@@ -1766,38 +1849,88 @@ void build_precond(Handle& H, cudaStream_t s) {
       std::sort(g.begin(), g.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
     const bool split = H.side != nullptr && !grp[0].empty() && !grp[1].empty();
     fork(split);
-    // right-looking, 64-column steps: diagonal blocks, panels, trailing update
+    // Two-level right-looking order (outer blocks of kOB2 columns, inner steps
+    // of 64).  Inside an outer block: the diagonal block of each inner step,
+    // its L21 for every row below and its U12 for the block's own columns, and
+    // the update of the block's own columns.  Then the columns right of the
+    // block: U12 = L11^{-1} A12 in four 64-row sub-steps (each applies the
+    // inner step's L^{-1}, then updates the block's rows below it), and the
+    // trailing matrix takes one kOB2-deep update.
     auto run_np = [&](const std::vector<int>& order, Handle::NpPlan& B, cudaStream_t st) {
       int gmax = 0;
       for (int l : order) gmax = std::max(gmax, 2 * rng[l].y);
-      struct Step {
-        int k0, d0, nd, p0, np, g0, ng;
+      struct Launch {
+        int kind;  // 0 diagonal, 1 panel, 2 update
+        int k0, depth, off, cnt, scr_slot0;
       };
-      std::vector<Step> steps;
+      std::vector<Launch> plan;
       std::vector<int> dl;
       std::vector<int4> pit, git;
+      const auto pack = [](int re, int ce) { return (re << 16) | ce; };
       int max_slots = 1;
-      for (int k0 = 0; k0 < gmax; k0 += kNP) {
-        Step st0{k0, (int)dl.size(), 0, (int)pit.size(), 0, (int)git.size(), 0};
-        int slot = 0;
+      auto emit = [&](int kind, int k0, int depth, size_t before, size_t after, int slot0) {
+        if (after > before)
+          plan.push_back({kind, k0, depth, (int)before, (int)(after - before), slot0});
+      };
+      for (int K0 = 0; K0 < gmax; K0 += kOB2) {
+        int nact = 0;
+        for (int l : order) nact += 2 * rng[l].y > K0;
+        max_slots = std::max(max_slots, nact);
+        // the leaves' rows in this outer block's diagonal launches: slot index
+        // = inner step * nact + position
+        for (int k0 = K0; k0 < std::min(gmax, K0 + kOB2); k0 += kNP) {
+          const int j = (k0 - K0) / kNP;
+          size_t d0 = dl.size(), p0 = pit.size(), g0 = git.size();
+          int slot = 0;
+          for (int l : order) {
+            const int m = 2 * rng[l].y;
+            if (m <= k0) continue;
+            dl.push_back(l);
+            const int d = std::min(kNP, m - k0), ce = std::min(m, K0 + kOB2);
+            for (int off = k0 + d; off < m; off += kNP)
+              pit.push_back(make_int4(l, j * nact + slot, 0, off));
+            for (int off = k0 + d; off < ce; off += kNP)
+              pit.push_back(make_int4(l, j * nact + slot, 1, off));
+            for (int r0 = k0 + d; r0 < m; r0 += kG2M)
+              for (int c0 = k0 + d; c0 < ce; c0 += kG2N)
+                git.push_back(make_int4(l, r0, c0, pack(m, ce)));
+            ++slot;
+          }
+          emit(0, k0, 0, d0, dl.size(), j * nact);
+          emit(1, k0, 0, p0, pit.size(), 0);
+          emit(2, k0, kNP, g0, git.size(), 0);
+        }
+        // the columns right of the block (leaves with m > K0 + kOB2 have all
+        // four inner steps; their slot in inner step j is j * nact + the
+        // leaf's position among the active leaves)
+        const int Kend = K0 + kOB2;
+        for (int j = 0; j < kOB2 / kNP; ++j) {
+          const int k0 = K0 + j * kNP;
+          size_t p0 = pit.size(), g0 = git.size();
+          int pos = 0;
+          for (int l : order) {
+            const int m = 2 * rng[l].y;
+            if (m <= K0) continue;
+            if (m > Kend) {
+              for (int off = Kend; off < m; off += kNP)
+                pit.push_back(make_int4(l, j * nact + pos, 1, off));
+              for (int r0 = k0 + kNP; r0 < Kend; r0 += kG2M)
+                for (int c0 = Kend; c0 < m; c0 += kG2N)
+                  git.push_back(make_int4(l, r0, c0, pack(Kend, m)));
+            }
+            ++pos;
+          }
+          emit(1, k0, 0, p0, pit.size(), 0);
+          emit(2, k0, kNP, g0, git.size(), 0);
+        }
+        size_t g0 = git.size();
         for (int l : order) {
           const int m = 2 * rng[l].y;
-          if (m <= k0) continue;
-          dl.push_back(l);
-          const int d = std::min(kNP, m - k0);
-          for (int off = k0 + d; off < m; off += kNP) {
-            pit.push_back(make_int4(l, slot, 0, off));
-            pit.push_back(make_int4(l, slot, 1, off));
-          }
-          for (int r0 = k0 + d; r0 < m; r0 += kG2M)
-            for (int c0 = k0 + d; c0 < m; c0 += kG2N) git.push_back(make_int4(l, r0, c0, 0));
-          ++slot;
+          if (m <= Kend) continue;
+          for (int r0 = Kend; r0 < m; r0 += kG2M)
+            for (int c0 = Kend; c0 < m; c0 += kG2N) git.push_back(make_int4(l, r0, c0, 0));
         }
-        max_slots = std::max(max_slots, slot);
-        st0.nd = (int)dl.size() - st0.d0;
-        st0.np = (int)pit.size() - st0.p0;
-        st0.ng = (int)git.size() - st0.g0;
-        steps.push_back(st0);
+        emit(2, K0, kOB2, g0, git.size(), 0);
       }
       auto up = [&](auto& buf, const auto& v) {
         buf.alloc(std::max<size_t>(v.size(), 1));
@@ -1808,22 +1941,23 @@ void build_precond(Handle& H, cudaStream_t s) {
       up(B.dleaves, dl);
       up(B.pitems, pit);
       up(B.gitems, git);
-      B.scr.alloc((size_t)max_slots * 2 * kNP * kNP);
-      for (const Step& q : steps) {
-        { TABI_K(K_LU, st);
-          lu_np_diag_kernel<<<q.nd, kNPT, kNPDiagSmem, st>>>(
-              B.dleaves.p + q.d0, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p, T.d_lu.p,
-              T.d_dinv.p, B.scr.p, d_fail.p); }
-        if (q.np > 0) {
+      B.scr.alloc((size_t)max_slots * (kOB2 / kNP) * 2 * kNP * kNP);
+      for (const Launch& q : plan) {
+        if (q.kind == 0) {
+          TABI_K(K_LU, st);
+          lu_np_diag_kernel<<<q.cnt, kNPT, kNPDiagSmem, st>>>(
+              B.dleaves.p + q.off, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p,
+              T.d_lu.p, T.d_dinv.p, B.scr.p + (size_t)q.scr_slot0 * 2 * kNP * kNP, d_fail.p);
+        } else if (q.kind == 1) {
           TABI_K(K_LU_STRIP, st);
-          lu_np_panel_kernel<<<q.np, kNPT, kNPPanelSmem, st>>>(
-              B.pitems.p + q.p0, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, B.scr.p,
+          lu_np_panel_kernel<<<q.cnt, kNPT, kNPPanelSmem, st>>>(
+              B.pitems.p + q.off, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, B.scr.p,
               d_fail.p);
-        }
-        if (q.ng > 0) {
+        } else {
           TABI_K(K_LU_UPDATE, st);
-          lu_gemm2_kernel<<<q.ng, 256, kGemm2Smem, st>>>(B.gitems.p + q.g0, q.k0,
-                                                         T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p);
+          lu_gemm2_kernel<<<q.cnt, 256, kGemm2Smem, st>>>(B.gitems.p + q.off, q.k0, q.depth,
+                                                          T.d_leaf_rng.p, T.d_blk_off.p,
+                                                          T.d_lu.p);
         }
       }
     };
@@ -2135,13 +2269,7 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
     TABI_CUDA(cudaEventRecord(H.ev_fork, s));
     TABI_CUDA(cudaStreamWaitEvent(s2, H.ev_fork, 0));
   }
-  if (nbig > 0 && 2 * T.max_leaf <= kSC * kSCT) {
-    // blocks of order 513..1024: a cluster of kSC CTAs per block
-    TABI_K(K_SOLVE, s);
-    solve_cluster_kernel<<<nbig * kSC, kSCT, 0, s>>>(T.d_leaf_rng.p, T.d_blk_off.p,
-                                                     T.d_dinv_off.p, list, T.d_lu.p, T.d_dinv.p,
-                                                     T.d_lu_perm.p, n, r, z);
-  } else if (nbig > 0) {
+  if (nbig > 0) {
     TABI_K(K_SOLVE, s);
     solve_kernel<512><<<nbig, 512, smem, s>>>(T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p,
                                               list, T.d_lu.p, T.d_dinv.p, T.d_lu_perm.p, n, r,
