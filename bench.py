@@ -217,6 +217,7 @@ def gpu_arm(args):
                               d["atmchr"].data_ptr(), None, sp)
 
     fp64_peak = tabipb.probe_fp64_peak(300.0)
+    fp32_peak = tabipb.probe_fp32_peak(300.0)
     for _ in range(args.warmup):
         res = step()
     flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > 126 MB L2
@@ -294,6 +295,30 @@ def gpu_arm(args):
                                     theta=w["theta"], kappa=kap, eps0=w["eps0"], eps1=w["eps1"],
                                     tol=w["tol"], precision=tabipb.PREC_MIXED)
         mixed = timed_leg(msolver)
+        # the FP32 treecode operator alone: its roofline against the FFMA peak
+        # and its interaction rate (the same interaction counts as FP64)
+        xm = torch.randn(2 * nface, dtype=torch.float64, device=dev)
+        ym = torch.empty_like(xm)
+        for _ in range(3):
+            msolver.matvec_dev(xm.data_ptr(), ym.data_ptr(), 2 * nface, sp)
+        ev = []
+        for _ in range(10):
+            a, b_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            msolver.matvec_dev(xm.data_ptr(), ym.data_ptr(), 2 * nface, sp)
+            b_.record(stream)
+            ev.append((a, b_))
+        torch.cuda.synchronize()
+        mv32_s = sum(a.elapsed_time(b_) for a, b_ in ev) / len(ev) / 1e3
+        ops32 = res["near_pairs"] * OPS_NEAR_PAIR + res["far"] * far_ops(w["order"])
+        mixed["roofline"] = {"kernel": "FP32 treecode matvec: near_kernel_f32 || "
+                                       "far_kernel<p, float> (+ moments, reduce)",
+                             "bound": "fp32", "achieved": ops32 / mv32_s / 1e12,
+                             "peak": fp32_peak / 1e12, "unit": "TFLOP/s",
+                             "frac": ops32 / mv32_s / fp32_peak,
+                             "peak_source": "FFMA loop probe (tabi_probe_fp32_peak), this GPU",
+                             "avg_launch_ms": mv32_s * 1e3}
+        mixed["matvec_interactions_per_s"] = (res["near_pairs"] + res["far"]) / mv32_s
         if os.path.exists(WEIGHTS):
             from tabipb.warmstart import WarmStart
 

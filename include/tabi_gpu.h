@@ -105,6 +105,17 @@ int tabi_form_matrix(tabi_h h, int nspt, const double* sptpos,
                      double* tr_xyz, double* tr_q, double* tr_area,
                      double* bvct);
 
+/* readin.f90:264-333 surface_area on device arrays: drops the faces whose
+ * Heron area is below 1e-5 or whose centroid lies within sqrt(1e-5) of one of
+ * the 10 faces before it in the given list.  nvert_dev: 3 x nface, 1-based;
+ * nvert_out_dev (capacity 3 x nface, not aliasing the input) receives the kept
+ * faces in their order, *nkept their number and *s_area the total area of all
+ * faces (summed by blocks: it differs from the reference's running sum in
+ * rounding only).  Returns after the counts are on the host. */
+int tabi_face_filter_dev(tabi_h h, int nspt, const double* sptpos_dev, int nface,
+                         const int* nvert_dev, int* nvert_out_dev, int* nkept,
+                         double* s_area, void* stream);
+
 /* Loads centroids, unit normals and areas (original order) when the caller
  * already has them (the state form_matrix leaves in module treecode). */
 int tabi_set_surface(tabi_h h, int nface, const double* tr_xyz,
@@ -226,6 +237,9 @@ const char* tabi_profile_class_name(int kclass);
 /* FP64 pipe peak probe: runs a DFMA loop for about `ms` milliseconds and
  * returns the achieved FP64 FLOP/s (2 per FMA). */
 int tabi_probe_fp64_peak(double ms, double* flops);
+/* The same for the FP32 pipe (FFMA loop), the denominator of the
+ * mixed-precision operator's roofline. */
+int tabi_probe_fp32_peak(double ms, double* flops);
 
 /* Accuracy reference (no counterpart in the reference, whose treecode is
  * checked against a direct sum only in its papers): the operator evaluated

@@ -248,6 +248,138 @@ void pack_atoms_dev(Handle& H, int nchr, const double* chrpos_dev, const double*
                                                           H.d_atoms.p); }
 }
 
+// ---- readin.f90:264-333 surface_area on the device.  A face is dropped when
+// its Heron area is below 1e-5 or its centroid lies within sqrt(1e-5) of the
+// centroid of any of the 10 faces before it in the ORIGINAL list (dropped
+// ones included), so every face decides alone: one flag kernel (recomputing
+// the 10 earlier centroids, with the reference's evaluation order), one
+// prefix over the blocks' counts, one order-preserving compaction.
+constexpr int kFFT = 256;  // faces per block
+
+__device__ __forceinline__ void face_centroid(const double* __restrict__ sptpos,
+                                              const int* __restrict__ nvert, int nspt, int f,
+                                              double (&c)[3], double (&v)[3][3], bool& bad) {
+  const double third = 1.0 / 3.0;
+  c[0] = c[1] = c[2] = 0.0;
+  for (int k = 0; k < 3; ++k) {
+    int id = nvert[3 * (size_t)f + k] - 1;
+    if (id < 0 || id >= nspt) {
+      bad = true;
+      id = 0;
+    }
+    for (int d = 0; d < 3; ++d) {
+      const double p = sptpos[3 * (size_t)id + d];
+      v[k][d] = p;
+      c[d] = __dadd_rn(c[d], __dmul_rn(third, p));
+    }
+  }
+}
+
+__global__ void __launch_bounds__(kFFT) face_flag_kernel(
+    const double* __restrict__ sptpos, int nspt, const int* __restrict__ nvert, int nface,
+    unsigned char* __restrict__ keep, int* __restrict__ bcount, double* __restrict__ barea,
+    int* __restrict__ bad_out) {
+  const int i = blockIdx.x * kFFT + threadIdx.x;
+  bool bad = false, k = false;
+  double area = 0.0;
+  if (i < nface) {
+    double c[3], v[3][3];
+    face_centroid(sptpos, nvert, nspt, i, c, v, bad);
+    area = heron(dist_rn(v[0], v[1]), dist_rn(v[0], v[2]), dist_rn(v[1], v[2]));
+    bool alert = false;
+    for (int ii = max(0, i - 10); ii < i; ++ii) {
+      double cc[3], vv[3][3];
+      face_centroid(sptpos, nvert, nspt, ii, cc, vv, bad);
+      double df[3] = {__dsub_rn(c[0], cc[0]), __dsub_rn(c[1], cc[1]), __dsub_rn(c[2], cc[2])};
+      if (dot3_rn(df, df) < 1e-5) alert = true;
+    }
+    k = !(area < 1e-5 || alert);
+    keep[i] = k ? 1 : 0;
+  }
+  if (bad) atomicExch(bad_out, 1);
+  // the block's kept count and its area sum (fixed-order tree: deterministic)
+  __shared__ double sa[kFFT];
+  __shared__ int sc[kFFT];
+  sa[threadIdx.x] = area;
+  sc[threadIdx.x] = k ? 1 : 0;
+  __syncthreads();
+  for (int w = kFFT / 2; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) {
+      sa[threadIdx.x] += sa[threadIdx.x + w];
+      sc[threadIdx.x] += sc[threadIdx.x + w];
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) {
+    bcount[blockIdx.x] = sc[0];
+    barea[blockIdx.x] = sa[0];
+  }
+}
+
+// exclusive prefix of the block counts (one thread, blocks in order), the
+// kept total and the total area
+__global__ void face_scan_kernel(int* __restrict__ bcount, const double* __restrict__ barea,
+                                 int nblk, int* __restrict__ total, double* __restrict__ s_area) {
+  if (threadIdx.x != 0) return;
+  int run = 0;
+  double a = 0.0;
+  for (int b = 0; b < nblk; ++b) {
+    const int c = bcount[b];
+    bcount[b] = run;
+    run += c;
+    a += barea[b];
+  }
+  *total = run;
+  *s_area = a;
+}
+
+__global__ void __launch_bounds__(kFFT) face_compact_kernel(const int* __restrict__ nvert,
+                                                           int nface,
+                                                           const unsigned char* __restrict__ keep,
+                                                           const int* __restrict__ boff,
+                                                           int* __restrict__ out) {
+  __shared__ int wsum[kFFT / 32];
+  const int i = blockIdx.x * kFFT + threadIdx.x;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const bool k = i < nface && keep[i];
+  const unsigned bal = __ballot_sync(0xffffffffu, k);
+  if (lane == 0) wsum[warp] = __popc(bal);
+  __syncthreads();
+  int before = 0;
+  for (int w = 0; w < warp; ++w) before += wsum[w];
+  if (k) {
+    const int pos = boff[blockIdx.x] + before + __popc(bal & ((1u << lane) - 1u));
+    out[3 * (size_t)pos] = nvert[3 * (size_t)i];
+    out[3 * (size_t)pos + 1] = nvert[3 * (size_t)i + 1];
+    out[3 * (size_t)pos + 2] = nvert[3 * (size_t)i + 2];
+  }
+}
+
+void face_filter_dev(Handle& H, int nspt, const double* sptpos, int nface, const int* nvert,
+                     int* nvert_out, int* nkept, double* s_area, cudaStream_t s) {
+  const int nblk = ceil_div(nface, kFFT);
+  H.ff_keep.alloc(nface);
+  H.ff_cnt.alloc(nblk + 2);
+  H.ff_area.alloc(nblk + 1);
+  TABI_CUDA(cudaMemsetAsync(H.ff_cnt.p + nblk, 0, 2 * sizeof(int), s));
+  { TABI_K(K_FORM, s);
+    face_flag_kernel<<<nblk, kFFT, 0, s>>>(sptpos, nspt, nvert, nface, H.ff_keep.p, H.ff_cnt.p,
+                                           H.ff_area.p, H.ff_cnt.p + nblk + 1); }
+  { TABI_K(K_FORM, s);
+    face_scan_kernel<<<1, 32, 0, s>>>(H.ff_cnt.p, H.ff_area.p, nblk, H.ff_cnt.p + nblk,
+                                      H.ff_area.p + nblk); }
+  { TABI_K(K_FORM, s);
+    face_compact_kernel<<<nblk, kFFT, 0, s>>>(nvert, nface, H.ff_keep.p, H.ff_cnt.p,
+                                              nvert_out); }
+  int hb[2];
+  TABI_CUDA(cudaMemcpyAsync(hb, H.ff_cnt.p + nblk, 2 * sizeof(int), cudaMemcpyDeviceToHost, s));
+  TABI_CUDA(cudaMemcpyAsync(s_area, H.ff_area.p + nblk, sizeof(double), cudaMemcpyDeviceToHost,
+                            s));
+  TABI_CUDA(cudaStreamSynchronize(s));
+  TABI_REQUIRE(hb[1] == 0, TABI_ERR_ARG, "face vertex index out of range");
+  *nkept = hb[0];
+}
+
 void launch_form_matrix(Handle& H, int nspt, const double* sptpos, const double* sptnrm,
                         int nface, const int* nvert, int nchr, const double* atoms4,
                         double* d_b, cudaStream_t s) {

@@ -111,10 +111,12 @@ __global__ void permute_b_kernel(const int* perm, int n, const double* b, double
   tb[n + i] = b[n + o];
 }
 
-__global__ void fp64_peak_kernel(double* out, long iters) {
-  double a0 = threadIdx.x * 1e-9, a1 = a0 + 1e-9, a2 = a0 + 2e-9, a3 = a0 + 3e-9;
-  double a4 = a0 + 4e-9, a5 = a0 + 5e-9, a6 = a0 + 6e-9, a7 = a0 + 7e-9;
-  const double m = 0.999999, c = 1e-7;
+// FMA peak probe: eight independent chains per thread (T = double or float)
+template <typename T>
+__global__ void fma_peak_kernel(T* out, long iters) {
+  T a0 = threadIdx.x * T(1e-9), a1 = a0 + T(1e-9), a2 = a0 + T(2e-9), a3 = a0 + T(3e-9);
+  T a4 = a0 + T(4e-9), a5 = a0 + T(5e-9), a6 = a0 + T(6e-9), a7 = a0 + T(7e-9);
+  const T m = T(0.999999), c = T(1e-7);
   for (long i = 0; i < iters; ++i) {
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
@@ -128,8 +130,41 @@ __global__ void fp64_peak_kernel(double* out, long iters) {
       a7 = fma(a7, m, c);
     }
   }
-  double s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
-  if (s == 123.456) out[0] = s;  // keeps the loop alive
+  T s = a0 + a1 + a2 + a3 + a4 + a5 + a6 + a7;
+  if (s == T(123.456)) out[0] = s;  // keeps the loop alive
+}
+
+template <typename T>
+int probe_fma_peak(double ms, double* flops) {
+  if (!flops) return TABI_ERR_ARG;
+  return guarded(nullptr, [&] {
+    int dev = 0, nsm = 0;
+    TABI_CUDA(cudaGetDevice(&dev));
+    TABI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+    DBuf<T> out;
+    out.alloc(1);
+    cudaEvent_t e0, e1;
+    TABI_CUDA(cudaEventCreate(&e0));
+    TABI_CUDA(cudaEventCreate(&e1));
+    int blocks = nsm * 8, threads = 256;
+    long iters = 64;
+    double t = 0.0;
+    for (int rep = 0; rep < 12; ++rep) {
+      TABI_CUDA(cudaEventRecord(e0));
+      fma_peak_kernel<T><<<blocks, threads>>>(out.p, iters);
+      TABI_CUDA(cudaEventRecord(e1));
+      TABI_CUDA(cudaEventSynchronize(e1));
+      float f = 0;
+      TABI_CUDA(cudaEventElapsedTime(&f, e0, e1));
+      t = f;
+      if (t >= ms) break;
+      iters = (long)(iters * std::min(8.0, std::max(1.5, ms / std::max(t, 1e-3))));
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    double fl = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    *flops = fl / (t * 1e-3);
+  });
 }
 
 void check_params(const tabi_params& p) {
@@ -645,6 +680,22 @@ int tabi_counts(tabi_h h, int64_t* near_pairs, int64_t* far_interactions) {
   });
 }
 
+int tabi_face_filter_dev(tabi_h h, int nspt, const double* sptpos_dev, int nface,
+                         const int* nvert_dev, int* nvert_out_dev, int* nkept, double* s_area,
+                         void* stream) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    Handle& H = h->H;
+    TABI_REQUIRE(nspt > 0 && nface > 0 && sptpos_dev && nvert_dev && nvert_out_dev && nkept &&
+                     s_area,
+                 TABI_ERR_ARG, "bad arguments");
+    TABI_REQUIRE(nvert_out_dev != nvert_dev, TABI_ERR_ARG, "the output must not alias the input");
+    set_device(H);
+    face_filter_dev(H, nspt, sptpos_dev, nface, nvert_dev, nvert_out_dev, nkept, s_area,
+                    pick(H, stream));
+  });
+}
+
 int tabi_pivoted_leaves(tabi_h h, int* count) {
   if (!h) return TABI_ERR_ARG;
   return guarded(h, [&] {
@@ -727,37 +778,8 @@ const char* tabi_profile_class_name(int kclass) {
   return (kclass >= 0 && kclass < K_NCLASS) ? names[kclass] : "all";
 }
 
-int tabi_probe_fp64_peak(double ms, double* flops) {
-  if (!flops) return TABI_ERR_ARG;
-  return guarded(nullptr, [&] {
-    int dev = 0, nsm = 0;
-    TABI_CUDA(cudaGetDevice(&dev));
-    TABI_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
-    DBuf<double> out;
-    out.alloc(1);
-    cudaEvent_t e0, e1;
-    TABI_CUDA(cudaEventCreate(&e0));
-    TABI_CUDA(cudaEventCreate(&e1));
-    int blocks = nsm * 8, threads = 256;
-    long iters = 64;
-    double t = 0.0;
-    for (int rep = 0; rep < 12; ++rep) {
-      TABI_CUDA(cudaEventRecord(e0));
-      fp64_peak_kernel<<<blocks, threads>>>(out.p, iters);
-      TABI_CUDA(cudaEventRecord(e1));
-      TABI_CUDA(cudaEventSynchronize(e1));
-      float f = 0;
-      TABI_CUDA(cudaEventElapsedTime(&f, e0, e1));
-      t = f;
-      if (t >= ms) break;
-      iters = (long)(iters * std::min(8.0, std::max(1.5, ms / std::max(t, 1e-3))));
-    }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    double fl = 2.0 * 8 * 16 * (double)iters * blocks * threads;
-    *flops = fl / (t * 1e-3);
-  });
-}
+int tabi_probe_fp64_peak(double ms, double* flops) { return probe_fma_peak<double>(ms, flops); }
+int tabi_probe_fp32_peak(double ms, double* flops) { return probe_fma_peak<float>(ms, flops); }
 
 // ---- accuracy reference
 int tabi_direct_targets(tabi_h h, int nt, const int* targets, const double* x, double* y) {

@@ -321,6 +321,10 @@ struct Handle {
   DBuf<double> st_pos, st_nrm, st_cp, st_q, st_b, st_axyz, st_aq, st_x;
   DBuf<int> st_fv;
   DBuf<double> rn_b0, rn_b, rn_x, rn_z;
+  // device face filter
+  DBuf<unsigned char> ff_keep;
+  DBuf<int> ff_cnt;
+  DBuf<double> ff_area;
   // output_potential
   DBuf<double> vp_cen, vp_xo, vp_vert, vp_pos;
   DBuf<int> vp_cnt, vp_off, vp_list, vp_err, vp_scan, vp_nv;
@@ -332,6 +336,10 @@ void launch_form_matrix(Handle& H, int nspt, const double* sptpos, const double*
                         int nface, const int* nvert, int nchr, const double* atoms4,
                         double* d_b, cudaStream_t s);
 void launch_rhs(Handle& H, int nchr, const double* atoms4, double* d_b, cudaStream_t s);
+// readin.f90:264-333 surface_area on device arrays: nvert_out (3 x nface
+// capacity) receives the kept faces in order; *nkept and *s_area on the host
+void face_filter_dev(Handle& H, int nspt, const double* sptpos, int nface, const int* nvert,
+                     int* nvert_out, int* nkept, double* s_area, cudaStream_t s);
 void energy_dev(Handle& H, int nchr, const double* chrpos, const double* atmchr, const double* x,
                 double* soleng, double* couleng, cudaStream_t s);
 // tree + lists (tree.cu)
@@ -355,8 +363,10 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s);
 void output_potential_dev(Handle& H, int nspt, const double* sptpos, int nface, const int* nvert,
                           const double* x, double* x_orig, double* vert_ptl, cudaStream_t s);
 // gmres (gmres.cu)
+// minv_b (may be null): M^-1 b already formed (device, 2n) and its norm
 void gmres_dev(Handle& H, const double* b, double* x, int* iter, double* err, int* ierr,
-               double* hist, int* nhist, cudaStream_t s, double tol = -1.0);
+               double* hist, int* nhist, cudaStream_t s, double tol = -1.0,
+               const double* minv_b = nullptr, double minv_b_nrm = 0.0);
 // the solve the handle's precision asks for: gmres_dev (FP64) or FP64 GMRES-IR
 // around FP32-operator GMRES (mixed)
 void solve_dev(Handle& H, const double* b, double* x, int* iter, double* err, int* ierr,

@@ -34,7 +34,8 @@ SYMBOLS = [
     "tabi_ws_set_params", "tabi_ws_predict_dev", "tabi_ws_loss_grad_dev",
     "tabi_ws_train_step_dev", "tabi_ws_graph_dev", "tabi_set_warmstart", "tabi_batch_run_dev",
     "tabi_output_potential", "tabi_output_potential_dev", "tabi_set_target_range",
-    "tabi_direct_targets", "tabi_pivoted_leaves",
+    "tabi_direct_targets", "tabi_pivoted_leaves", "tabi_probe_fp32_peak",
+    "tabi_face_filter_dev",
 ]
 
 
@@ -107,6 +108,8 @@ def load(path: str = LIB_PATH):
     L.tabi_counts.argtypes = [_vp, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.tabi_tree_nodes.argtypes = [_vp, _ip, _ip, _ip, _ip, _ip, _dp]
     L.tabi_probe_fp64_peak.argtypes = [C.c_double, _dp]
+    L.tabi_probe_fp32_peak.argtypes = [C.c_double, _dp]
+    L.tabi_face_filter_dev.argtypes = [_vp, C.c_int, _vp, C.c_int, _vp, _vp, _ip, _dp, _vp]
     L.tabi_profile_enable.argtypes = [_vp, C.c_int]
     L.tabi_profile_read.argtypes = [_vp, C.c_int, _dp, C.POINTER(C.c_int64)]
     L.tabi_profile_nclasses.argtypes = []

@@ -268,6 +268,15 @@ class TabiSolver:
     def matvec_dev(self, x_ptr, y_ptr, n2, stream=None):
         check(self.h, self.L.tabi_matvec_dev(self.h, n2, x_ptr, y_ptr, stream))
 
+    def face_filter_dev(self, nspt, sptpos_ptr, nface, nvert_ptr, nvert_out_ptr, stream=None):
+        """readin.f90:264-333 on device arrays (tabi_face_filter_dev): returns
+        (kept face count, total area); the kept faces go to nvert_out_ptr."""
+        nk, sa = C.c_int(), C.c_double()
+        check(self.h, self.L.tabi_face_filter_dev(self.h, nspt, sptpos_ptr, nface, nvert_ptr,
+                                                  nvert_out_ptr, C.byref(nk), C.byref(sa),
+                                                  stream))
+        return nk.value, sa.value
+
     def set_warmstart(self, ws):
         """Attach a warmstart.WarmStart (None detaches): run_dev then starts
         GMRES from the network's prediction (tabi_set_warmstart)."""
@@ -290,6 +299,14 @@ def probe_fp64_peak(ms=200.0) -> float:
     rc = _lib.load().tabi_probe_fp64_peak(ms, C.byref(f))
     if rc != 0:
         raise TabiError(rc, "fp64 probe failed")
+    return f.value
+
+
+def probe_fp32_peak(ms=200.0) -> float:
+    f = C.c_double()
+    rc = _lib.load().tabi_probe_fp32_peak(ms, C.byref(f))
+    if rc != 0:
+        raise TabiError(rc, "fp32 probe failed")
     return f.value
 
 
