@@ -602,6 +602,15 @@ def batched_leg(args, dev, rank):
     if t_par > t_seq:  # the subset's choice did not carry over: one worker ran faster
         nw, par, t_par = 1, seq, t_seq
     ok = bool(np.all(par[:, 2] == 0)) and bool(np.array_equal(seq[:, 3], par[:, 3]))
+    # each molecule's solvation energy against its own plain solve (FP64,
+    # leaf 500, no warm start, the same tol): the error of the accelerated
+    # configuration (FP32 treecode + refinement, tuned leaf size, warm start)
+    prm64 = tabipb.default_params(order=w["order"], theta=w["theta"],
+                                  maxparnode=w["maxparnode"],
+                                  kappa=tabipb.kappa(w["bulk"], w["eps1"]), eps0=w["eps0"],
+                                  eps1=w["eps1"], tol=w["tol"], precision=tabipb.PREC_FP64)
+    ref64, _ = B.run_batch(mols, prm64, ws=None, nworkers=nw, table=None)
+    dg_err = np.abs(par[:, 3] - ref64[:, 3]) / np.abs(ref64[:, 3])
     return {"value": len(mols) / t_par, "unit": "molecules/s", "molecules": len(mols),
             "workers": nw, "tuned_workers": tuned_workers,
             "worker_tuning_s": {str(k): round(v, 4) for k, v in wt.items()},
@@ -615,6 +624,9 @@ def batched_leg(args, dev, rank):
             "per_molecule_ms_p50": float(np.percentile(par[:, 8], 50)),
             "per_molecule_ms_p99": float(np.percentile(par[:, 8], 99)),
             "all_converged_and_equal_to_sequential": ok,
+            "dG_rel_err_vs_plain_fp64_leaf500": {"max": float(dg_err.max()),
+                                                 "p99": float(np.percentile(dg_err, 99)),
+                                                 "median": float(np.median(dg_err))},
             "timing": "host wall clock around the whole batch call (inputs on the device), "
                       "best of 3 calls",
             "surface_generation_s": t_gen}
