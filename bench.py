@@ -243,6 +243,13 @@ def gpu_arm(args):
     ms = sum(a.elapsed_time(b) for a, b in times)
     prof = solver.profile_read()
     solver.profile(False)
+    # the leaf blocks' orders m = 2 x leaf size: the factorisation's work
+    # (2/3 m^3 flops per block, DGETRF's leading term) and the factor bytes
+    # one apply streams (m^2 doubles per block, plus its 32 x 32 inverse
+    # diagonal blocks)
+    leaf_m = 2 * solver.leaves()[1].astype(np.float64)
+    lu_flop = float((2.0 / 3.0 * leaf_m ** 3).sum())
+    apply_bytes = float(8 * (leaf_m ** 2).sum() + 8 * (np.ceil(leaf_m / 32) * 2 * 32 * 32).sum())
     ms_t = torch.tensor([ms], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
@@ -434,6 +441,8 @@ def gpu_arm(args):
                                           "far_interaction": far_ops(WORKLOAD["order"])},
                          "near_kernel_avg_ms": near_ms / max(near_n, 1),
                          "far_kernel_avg_ms": far_ms / max(far_n, 1)},
+            "lu": lu_entry(prof, lu_flop, fp64_peak),
+            "apply": apply_entry(prof, apply_bytes),
             "e2e": {"value": world / e2e_s, "unit": "solves/s", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h},
             "gpu_launches": int(prof["all"][1]),
@@ -540,6 +549,41 @@ def _batch_surface(job):
     pos, nrm, fc, _ = S.gaussian_surface(xyz, r, density=density, probe=1.4)
     fc, _ = S.face_filter(pos, fc)
     return natm, seed, pos, nrm, fc, xyz, q
+
+
+def hbm_peak_gbs():
+    """The measured copy bandwidth of this pool's B200s (the driver-written
+    peaks file at the repository root), else the earlier pool measurement."""
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback (6.65 TB/s, earlier pool measurement)"
+
+
+def lu_entry(prof, lu_flop, fp64_peak):
+    """The leaf-block factorisation's FP64 rate: its work over the span from
+    its first launch to the join of both LU streams (library event timer)."""
+    ms, n = prof.get("lu", (0.0, 0))
+    if n <= 0 or ms <= 0:
+        return None
+    t = ms / n
+    return {"flop_per_factorisation": lu_flop, "ms": t, "tflops": lu_flop / t / 1e9,
+            "frac_of_fp64_peak": lu_flop / t / 1e9 / (fp64_peak / 1e12),
+            "timing": "CUDA events around the factorisation (both streams), mean over the timed steps"}
+
+
+def apply_entry(prof, apply_bytes):
+    """The preconditioner apply's streaming rate against the HBM peak: the
+    factor bytes over one apply's span (fork to join)."""
+    ms, n = prof.get("apply", (0.0, 0))
+    if n <= 0 or ms <= 0:
+        return None
+    peak, src = hbm_peak_gbs()
+    t = ms / n
+    return {"bytes_per_apply": apply_bytes, "us": t * 1e3, "gbs": apply_bytes / t / 1e6,
+            "frac_of_hbm": apply_bytes / t / 1e6 / peak, "hbm_peak_gbs": peak,
+            "peak_source": src, "applies_per_step": n / max(prof.get("lu", (0, 1))[1], 1)}
 
 
 def batched_leg(args, dev, rank):

@@ -15,6 +15,7 @@
 // (right-looking LU with partial pivoting, the same pivot rule, batched over
 // all leaves) and every apply is a blocked forward/back substitution.
 #include <algorithm>
+#include <optional>
 #include <climits>
 
 #include "bie_kernels.cuh"
@@ -1821,6 +1822,8 @@ void build_precond(Handle& H, cudaStream_t s) {
     TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
   };
   // ---- unpivoted factorisation of every leaf, certified (see lu_np_diag_kernel)
+  std::optional<KScope> lu_phase;
+  lu_phase.emplace(H.prof, K_PHASE_LU, s);
   std::vector<int> pv_leaves;  // leaves factored with partial pivoting
   const bool try_np = (H.prm.flags & TABI_FLAG_PIVOTED_LU) == 0;
   if (try_np) {
@@ -2223,6 +2226,7 @@ void build_precond(Handle& H, cudaStream_t s) {
                                            " (coincident faces or non-finite surface data)");
     }
   }
+  lu_phase.reset();
   // apply lists: blocks of order > 512 get 512 threads (one wave on the GPU),
   // the others 256 threads on the side stream; largest first in each
   {
@@ -2251,6 +2255,7 @@ void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s) {
     TABI_CUDA(cudaGetLastError());
     return;
   }
+  TABI_PHASE(K_PHASE_APPLY, s);
   // two arrays of the block order m = 2 * leaf size, 32 doubles per warp and
   // two staged 32 x 32 inverse diagonal blocks
   size_t smem = sizeof(double) * (4 * (size_t)T.max_leaf + 512 + 2 * kDB * kDB);

@@ -758,7 +758,7 @@ int tabi_profile_read(tabi_h h, int kclass, double* ms, int64_t* launches) {
     double t = 0.0;
     int64_t l = 0;
     for (int k = 0; k < K_NCLASS; ++k)
-      if ((kclass == -1 && k != K_PHASE_MATVEC) || kclass == k) {
+      if ((kclass == -1 && k < K_PHASE_MATVEC) || kclass == k) {
         t += H.prof.ms[k];
         l += H.prof.launches[k];
       }
@@ -774,7 +774,7 @@ const char* tabi_profile_class_name(int kclass) {
                                         "far",         "near",   "reduce",    "assemble",
                                         "lu_panel",    "solve",  "vector",    "energy",
                                         "lu_update",   "lu_post",   "lu_strip",
-                                        "lu_swap",     "matvec"};
+                                        "lu_swap",     "matvec", "lu",       "apply"};
   return (kclass >= 0 && kclass < K_NCLASS) ? names[kclass] : "all";
 }
 

@@ -171,6 +171,8 @@ enum KClass {
   K_FORM = 0, K_TREE, K_LISTS, K_MOMENTS, K_FAR, K_NEAR, K_REDUCE, K_ASSEMBLE, K_LU,
   K_SOLVE, K_VEC, K_ENERGY, K_LU_UPDATE, K_LU_POST, K_LU_STRIP, K_LU_SWAP,
   K_PHASE_MATVEC,  // whole treecode matvec (a phase: timed, not a launch)
+  K_PHASE_LU,      // the leaf-block factorisation, first LU launch to the join of both streams
+  K_PHASE_APPLY,   // one preconditioner apply, fork to join
   K_NCLASS
 };
 
