@@ -1293,6 +1293,8 @@ __global__ void __launch_bounds__(kNPT) lu_np_diag_kernel(
     double* __restrict__ lu, double* __restrict__ dinv, double* __restrict__ scr,
     int* __restrict__ fail) {
   extern __shared__ double nsm[];
+  chain_wait();  // the previous launch of the chain has finished
+  chain_signal();
   double(*D)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm);
   double(*Li)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm + kNP * kNPPitch);
   double(*Ui)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm + 2 * kNP * kNPPitch);
@@ -1544,6 +1546,8 @@ __global__ void __launch_bounds__(kNPT) lu_np_panel_kernel(
     const int64_t* __restrict__ blk_off, double* __restrict__ lu,
     const double* __restrict__ scr, int* __restrict__ fail) {
   extern __shared__ double nsm[];
+  chain_wait();  // the previous launch of the chain has finished
+  chain_signal();
   double(*X)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm);
   double(*V)[kNPPitch] = reinterpret_cast<double(*)[kNPPitch]>(nsm + kNP * kNPPitch);
   const int4 it = items[blockIdx.x];
@@ -1639,6 +1643,8 @@ __global__ void __launch_bounds__(256, 2) lu_gemm2_kernel(const int4* __restrict
                                                           const int64_t* __restrict__ blk_off,
                                                           double* __restrict__ lu) {
   extern __shared__ double gsm2[];
+  chain_wait();  // the previous launch of the chain has finished
+  chain_signal();
   double* sL = gsm2;                      // [2][kG2K][kG2M]  L slice, k-major
   double* sU = gsm2 + 2 * kG2K * kG2M;    // [2][kG2N][kG2UP] U slice, by column
   const int4 it = items[blockIdx.x];
@@ -1778,30 +1784,30 @@ void build_precond(Handle& H, cudaStream_t s) {
   std::vector<int2> rng(nl);
   T.blk_off.resize(nl);
   int64_t off = 0;
-  std::vector<int2> tiles;
+  PinVec<int2>& tiles = H.pc_h_tiles;
+  tiles.begin();
   for (int l = 0; l < nl; ++l) {
     int c = T.leaves[l];
     rng[l] = make_int2(T.ibeg[c], T.num[c]);
     T.blk_off[l] = off;
     off += 4LL * T.num[c] * T.num[c];
-    for (int j = 0; j < T.num[c]; j += kAsmCols) tiles.push_back(make_int2(l, j));
+    for (int j = 0; j < T.num[c]; j += kAsmCols) tiles.push(make_int2(l, j));
   }
   T.d_lu.alloc(std::max<int64_t>(off, 1));
   T.d_piv.alloc(2 * (size_t)H.n);
   T.d_blk_off.alloc(nl);
   T.d_leaf_rng.alloc(nl);
   DBuf<int2>& d_tiles = H.pc_tiles;
-  d_tiles.alloc(tiles.size());
+  d_tiles.alloc(tiles.len);
   DBuf<int>& d_info = H.pc_info;
   d_info.alloc(nl);
-  TABI_CUDA(cudaMemcpyAsync(T.d_blk_off.p, T.blk_off.data(), sizeof(int64_t) * nl,
-                            cudaMemcpyHostToDevice, s));
-  TABI_CUDA(cudaMemcpyAsync(T.d_leaf_rng.p, rng.data(), sizeof(int2) * nl, cudaMemcpyHostToDevice,
-                            s));
-  TABI_CUDA(cudaMemcpyAsync(d_tiles.p, tiles.data(), sizeof(int2) * tiles.size(),
-                            cudaMemcpyHostToDevice, s));
+  H.pc_h_blk_off.assign(T.blk_off.data(), nl);
+  H.pc_h_blk_off.upload(T.d_blk_off, s);
+  H.pc_h_rng.assign(rng.data(), nl);
+  H.pc_h_rng.upload(T.d_leaf_rng, s);
+  tiles.upload(d_tiles, s);
   double eps = H.prm.eps1 / H.prm.eps0;
-  { TABI_K(K_ASSEMBLE, s); assemble_kernel<<<(int)tiles.size(), 256, 0, s>>>(d_tiles.p, T.d_leaf_rng.p, T.d_blk_off.p,
+  { TABI_K(K_ASSEMBLE, s); assemble_kernel<<<(int)tiles.len, 256, 0, s>>>(d_tiles.p, T.d_leaf_rng.p, T.d_blk_off.p,
                                                     H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p,
                                                     H.d_ny.p, H.d_nz.p, H.d_area.p,
                                                     H.prm.kappa, eps, T.d_lu.p); }
@@ -1841,8 +1847,8 @@ void build_precond(Handle& H, cudaStream_t s) {
     }
     T.d_dinv.alloc(std::max<int64_t>(doff, 1));
     T.d_dinv_off.alloc(nl);
-    TABI_CUDA(cudaMemcpyAsync(T.d_dinv_off.p, T.dinv_off.data(), sizeof(int64_t) * nl,
-                              cudaMemcpyHostToDevice, s));
+    H.pc_h_dinv_off.assign(T.dinv_off.data(), nl);
+    H.pc_h_dinv_off.upload(T.d_dinv_off, s);
     raise_smem_limit((const void*)lu_np_diag_kernel, kNPDiagSmem);
     raise_smem_limit((const void*)lu_np_panel_kernel, kNPPanelSmem);
     raise_smem_limit((const void*)lu_gemm2_kernel, kGemm2Smem);
@@ -1850,8 +1856,10 @@ void build_precond(Handle& H, cudaStream_t s) {
     for (int l = 0; l < nl; ++l) grp[2 * rng[l].y > kLuSmallBlock ? 0 : 1].push_back(l);
     for (auto& g : grp)
       std::sort(g.begin(), g.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
-    const bool split = H.side != nullptr && !grp[0].empty() && !grp[1].empty();
-    fork(split);
+    // both groups on the handle's high-priority LU streams, forked from s
+    TABI_CUDA(cudaEventRecord(H.ev_fork, s));
+    TABI_CUDA(cudaStreamWaitEvent(H.lu_hi, H.ev_fork, 0));
+    TABI_CUDA(cudaStreamWaitEvent(H.lu_small, H.ev_fork, 0));
     // Two-level right-looking order (outer blocks of kOB2 columns, inner steps
     // of 64).  Inside an outer block: the diagonal block of each inner step,
     // its L21 for every row below and its U12 for the block's own columns, and
@@ -1859,22 +1867,40 @@ void build_precond(Handle& H, cudaStream_t s) {
     // block: U12 = L11^{-1} A12 in four 64-row sub-steps (each applies the
     // inner step's L^{-1}, then updates the block's rows below it), and the
     // trailing matrix takes one kOB2-deep update.
-    auto run_np = [&](const std::vector<int>& order, Handle::NpPlan& B, cudaStream_t st) {
+    //
+    // Look-ahead (the large-block group): the trailing update of an outer
+    // block is split by columns.  The next outer block's kOB2 columns, which
+    // its steps factor, are updated on the group's stream; the columns beyond
+    // it on the low-priority auxiliary stream, beside the next
+    // block's diagonal, panel and update launches, which touch only rows and
+    // columns of that block or its own columns below it.  The next block's
+    // columns right of it (rows of the block, columns beyond) wait for the
+    // auxiliary stream.  Every entry is updated by the same tile in the same
+    // k order as without the split, so the factors are the same bit for bit.
+    auto run_np = [&](const std::vector<int>& order, Handle::NpPlan& B, cudaStream_t st,
+                      bool la) {
       int gmax = 0;
       for (int l : order) gmax = std::max(gmax, 2 * rng[l].y);
       struct Launch {
-        int kind;  // 0 diagonal, 1 panel, 2 update
+        // 0 diagonal, 1 panel, 2 update, 3 fork to the auxiliary stream,
+        // 4 wait for the auxiliary stream, 5 update on the auxiliary stream
+        int kind;
         int k0, depth, off, cnt, scr_slot0;
       };
       std::vector<Launch> plan;
-      std::vector<int> dl;
-      std::vector<int4> pit, git;
+      PinVec<int>& dl = B.h_dleaves;
+      PinVec<int4>& pit = B.h_pitems;
+      PinVec<int4>& git = B.h_gitems;
+      dl.begin();
+      pit.begin();
+      git.begin();
       const auto pack = [](int re, int ce) { return (re << 16) | ce; };
       int max_slots = 1;
       auto emit = [&](int kind, int k0, int depth, size_t before, size_t after, int slot0) {
         if (after > before)
           plan.push_back({kind, k0, depth, (int)before, (int)(after - before), slot0});
       };
+      bool rest_pending = false;  // an update on the auxiliary stream not yet waited for
       for (int K0 = 0; K0 < gmax; K0 += kOB2) {
         int nact = 0;
         for (int l : order) nact += 2 * rng[l].y > K0;
@@ -1883,90 +1909,129 @@ void build_precond(Handle& H, cudaStream_t s) {
         // = inner step * nact + position
         for (int k0 = K0; k0 < std::min(gmax, K0 + kOB2); k0 += kNP) {
           const int j = (k0 - K0) / kNP;
-          size_t d0 = dl.size(), p0 = pit.size(), g0 = git.size();
+          size_t d0 = dl.len, p0 = pit.len, g0 = git.len;
           int slot = 0;
           for (int l : order) {
             const int m = 2 * rng[l].y;
             if (m <= k0) continue;
-            dl.push_back(l);
+            dl.push(l);
             const int d = std::min(kNP, m - k0), ce = std::min(m, K0 + kOB2);
             for (int off = k0 + d; off < m; off += kNP)
-              pit.push_back(make_int4(l, j * nact + slot, 0, off));
+              pit.push(make_int4(l, j * nact + slot, 0, off));
             for (int off = k0 + d; off < ce; off += kNP)
-              pit.push_back(make_int4(l, j * nact + slot, 1, off));
+              pit.push(make_int4(l, j * nact + slot, 1, off));
             for (int r0 = k0 + d; r0 < m; r0 += kG2M)
               for (int c0 = k0 + d; c0 < ce; c0 += kG2N)
-                git.push_back(make_int4(l, r0, c0, pack(m, ce)));
+                git.push(make_int4(l, r0, c0, pack(m, ce)));
             ++slot;
           }
-          emit(0, k0, 0, d0, dl.size(), j * nact);
-          emit(1, k0, 0, p0, pit.size(), 0);
-          emit(2, k0, kNP, g0, git.size(), 0);
+          emit(0, k0, 0, d0, dl.len, j * nact);
+          emit(1, k0, 0, p0, pit.len, 0);
+          emit(2, k0, kNP, g0, git.len, 0);
         }
         // the columns right of the block (leaves with m > K0 + kOB2 have all
         // four inner steps; their slot in inner step j is j * nact + the
         // leaf's position among the active leaves)
         const int Kend = K0 + kOB2;
+        if (rest_pending) {
+          plan.push_back({4, K0, 0, 0, 0, 0});
+          rest_pending = false;
+        }
         for (int j = 0; j < kOB2 / kNP; ++j) {
           const int k0 = K0 + j * kNP;
-          size_t p0 = pit.size(), g0 = git.size();
+          size_t p0 = pit.len, g0 = git.len;
           int pos = 0;
           for (int l : order) {
             const int m = 2 * rng[l].y;
             if (m <= K0) continue;
             if (m > Kend) {
               for (int off = Kend; off < m; off += kNP)
-                pit.push_back(make_int4(l, j * nact + pos, 1, off));
+                pit.push(make_int4(l, j * nact + pos, 1, off));
               for (int r0 = k0 + kNP; r0 < Kend; r0 += kG2M)
                 for (int c0 = Kend; c0 < m; c0 += kG2N)
-                  git.push_back(make_int4(l, r0, c0, pack(Kend, m)));
+                  git.push(make_int4(l, r0, c0, pack(Kend, m)));
             }
             ++pos;
           }
-          emit(1, k0, 0, p0, pit.size(), 0);
-          emit(2, k0, kNP, g0, git.size(), 0);
+          emit(1, k0, 0, p0, pit.len, 0);
+          emit(2, k0, kNP, g0, git.len, 0);
         }
-        size_t g0 = git.size();
+        // the trailing update: columns [Kend, Knext) here, the rest on the
+        // auxiliary stream (all of it here without look-ahead)
+        const int Knext = la ? Kend + kOB2 : INT_MAX;
+        size_t g0 = git.len;
         for (int l : order) {
           const int m = 2 * rng[l].y;
           if (m <= Kend) continue;
           for (int r0 = Kend; r0 < m; r0 += kG2M)
-            for (int c0 = Kend; c0 < m; c0 += kG2N) git.push_back(make_int4(l, r0, c0, 0));
+            for (int c0 = Kend; c0 < std::min(m, Knext); c0 += kG2N)
+              git.push(make_int4(l, r0, c0, 0));
         }
-        emit(2, K0, kOB2, g0, git.size(), 0);
+        const size_t g1 = git.len;
+        for (int l : order) {
+          const int m = 2 * rng[l].y;
+          if (m <= Knext) continue;
+          for (int r0 = Kend; r0 < m; r0 += kG2M)
+            for (int c0 = Knext; c0 < m; c0 += kG2N) git.push(make_int4(l, r0, c0, 0));
+        }
+        // the fork before the look-ahead columns' launch (the auxiliary stream
+        // must not wait for it), the rest launched after it (earlier launches
+        // are dispatched first)
+        const bool rest = git.len > g1;
+        if (rest) plan.push_back({3, K0, 0, 0, 0, 0});
+        emit(2, K0, kOB2, g0, g1, 0);
+        if (rest) {
+          emit(5, K0, kOB2, g1, git.len, 0);
+          rest_pending = true;
+        }
       }
-      auto up = [&](auto& buf, const auto& v) {
-        buf.alloc(std::max<size_t>(v.size(), 1));
-        if (!v.empty())
-          TABI_CUDA(cudaMemcpyAsync(buf.p, v.data(), sizeof(v[0]) * v.size(),
-                                    cudaMemcpyHostToDevice, st));
-      };
-      up(B.dleaves, dl);
-      up(B.pitems, pit);
-      up(B.gitems, git);
+      if (rest_pending) plan.push_back({4, gmax, 0, 0, 0, 0});
+      dl.upload(B.dleaves, st);
+      pit.upload(B.pitems, st);
+      git.upload(B.gitems, st);
       B.scr.alloc((size_t)max_slots * (kOB2 / kNP) * 2 * kNP * kNP);
+      // kernels follow kernels on `st` as a programmatic chain; the first one
+      // after the uploads or a cross-stream event starts the ordinary way
+      bool chain = false;
       for (const Launch& q : plan) {
         if (q.kind == 0) {
           TABI_K(K_LU, st);
-          lu_np_diag_kernel<<<q.cnt, kNPT, kNPDiagSmem, st>>>(
-              B.dleaves.p + q.off, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_dinv_off.p,
-              T.d_lu.p, T.d_dinv.p, B.scr.p + (size_t)q.scr_slot0 * 2 * kNP * kNP, d_fail.p);
+          launch_chained(chain, lu_np_diag_kernel, dim3(q.cnt), dim3(kNPT), kNPDiagSmem, st,
+                         B.dleaves.p + q.off, q.k0, T.d_leaf_rng.p, T.d_blk_off.p,
+                         T.d_dinv_off.p, T.d_lu.p, T.d_dinv.p,
+                         B.scr.p + (size_t)q.scr_slot0 * 2 * kNP * kNP, d_fail.p);
+          chain = true;
         } else if (q.kind == 1) {
           TABI_K(K_LU_STRIP, st);
-          lu_np_panel_kernel<<<q.cnt, kNPT, kNPPanelSmem, st>>>(
-              B.pitems.p + q.off, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p, B.scr.p,
-              d_fail.p);
+          launch_chained(chain, lu_np_panel_kernel, dim3(q.cnt), dim3(kNPT), kNPPanelSmem, st,
+                         B.pitems.p + q.off, q.k0, T.d_leaf_rng.p, T.d_blk_off.p, T.d_lu.p,
+                         B.scr.p, d_fail.p);
+          chain = true;
+        } else if (q.kind == 3) {
+          TABI_CUDA(cudaEventRecord(H.ev_la, st));
+          TABI_CUDA(cudaStreamWaitEvent(H.aux, H.ev_la, 0));
+          chain = false;
+        } else if (q.kind == 4) {
+          TABI_CUDA(cudaStreamWaitEvent(st, H.ev_rest, 0));
+          chain = false;
         } else {
-          TABI_K(K_LU_UPDATE, st);
-          lu_gemm2_kernel<<<q.cnt, 256, kGemm2Smem, st>>>(B.gitems.p + q.off, q.k0, q.depth,
-                                                          T.d_leaf_rng.p, T.d_blk_off.p,
-                                                          T.d_lu.p);
+          cudaStream_t gs = q.kind == 5 ? H.aux : st;
+          TABI_K(K_LU_UPDATE, gs);
+          launch_chained(chain && q.kind == 2, lu_gemm2_kernel, dim3(q.cnt), dim3(256),
+                         kGemm2Smem, gs,
+                         B.gitems.p + q.off, q.k0, q.depth, T.d_leaf_rng.p, T.d_blk_off.p,
+                         T.d_lu.p);
+          if (q.kind == 5) TABI_CUDA(cudaEventRecord(H.ev_rest, H.aux));
+          else chain = true;
         }
       }
     };
-    if (!grp[0].empty()) run_np(grp[0], H.pc_np[0], s);
-    if (!grp[1].empty()) run_np(grp[1], H.pc_np[1], split ? H.side : s);
-    join(split);
+    if (!grp[0].empty()) run_np(grp[0], H.pc_np[0], H.lu_hi, true);
+    if (!grp[1].empty()) run_np(grp[1], H.pc_np[1], H.lu_small, false);
+    TABI_CUDA(cudaEventRecord(H.ev_join, H.lu_small));
+    TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
+    TABI_CUDA(cudaEventRecord(H.ev_lu_join, H.lu_hi));
+    TABI_CUDA(cudaStreamWaitEvent(s, H.ev_lu_join, 0));
     std::vector<int> failed(nl);
     TABI_CUDA(cudaMemcpyAsync(failed.data(), d_fail.p, sizeof(int) * nl, cudaMemcpyDeviceToHost,
                               s));
@@ -2237,10 +2302,8 @@ void build_precond(Handle& H, cudaStream_t s) {
     T.n_solve_big = (int)big.size();
     T.n_solve_small = (int)small.size();
     big.insert(big.end(), small.begin(), small.end());
-    T.d_solve_list.alloc(std::max<size_t>(big.size(), 1));
-    TABI_CUDA(cudaMemcpyAsync(T.d_solve_list.p, big.data(), sizeof(int) * big.size(),
-                              cudaMemcpyHostToDevice, s));
-    TABI_CUDA(cudaStreamSynchronize(s));
+    H.pc_h_solve_list.assign(big.data(), big.size());
+    H.pc_h_solve_list.upload(T.d_solve_list, s);
   }
   H.has_precond = true;
 }

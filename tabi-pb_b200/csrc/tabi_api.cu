@@ -374,6 +374,18 @@ int tabi_create(tabi_h* h, const tabi_params* p) {
     TABI_CUDA(cudaStreamCreateWithFlags(&nh->H.side, cudaStreamNonBlocking));
     TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_fork, cudaEventDisableTiming));
     TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_join, cudaEventDisableTiming));
+    int prio_lo = 0, prio_hi = 0;
+    TABI_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
+    // the large-block chain first, then the trailing updates beside it (the
+    // chain waits for them one outer block later), then the small-block group
+    // (a short chain of its own that ends long before the large one)
+    TABI_CUDA(cudaStreamCreateWithPriority(&nh->H.lu_hi, cudaStreamNonBlocking, prio_hi));
+    TABI_CUDA(cudaStreamCreateWithPriority(&nh->H.aux, cudaStreamNonBlocking,
+                                           (prio_lo + prio_hi) / 2));
+    TABI_CUDA(cudaStreamCreateWithPriority(&nh->H.lu_small, cudaStreamNonBlocking, prio_lo));
+    TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_la, cudaEventDisableTiming));
+    TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_rest, cudaEventDisableTiming));
+    TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_lu_join, cudaEventDisableTiming));
     TABI_CUDA(cudaMallocHost(&nh->H.h_pinned, sizeof(double) * 256));
   });
   if (rc != TABI_OK) {
@@ -390,13 +402,15 @@ int tabi_destroy(tabi_h h) {
   if (h->H.stream) cudaStreamSynchronize(h->H.stream);
   if (h->H.h_pinned) cudaFreeHost(h->H.h_pinned);
   if (h->H.side) cudaStreamSynchronize(h->H.side);
-  cudaStream_t s = h->H.stream, s2 = h->H.side;
-  cudaEvent_t e1 = h->H.ev_fork, e2 = h->H.ev_join;
+  for (cudaStream_t x : {h->H.aux, h->H.lu_hi, h->H.lu_small})
+    if (x) cudaStreamSynchronize(x);
+  cudaStream_t st[] = {h->H.stream, h->H.side, h->H.aux, h->H.lu_hi, h->H.lu_small};
+  cudaEvent_t ev[] = {h->H.ev_fork, h->H.ev_join, h->H.ev_la, h->H.ev_rest, h->H.ev_lu_join};
   delete h;
-  if (s) cudaStreamDestroy(s);
-  if (s2) cudaStreamDestroy(s2);
-  if (e1) cudaEventDestroy(e1);
-  if (e2) cudaEventDestroy(e2);
+  for (cudaStream_t x : st)
+    if (x) cudaStreamDestroy(x);
+  for (cudaEvent_t x : ev)
+    if (x) cudaEventDestroy(x);
   return TABI_OK;
 }
 

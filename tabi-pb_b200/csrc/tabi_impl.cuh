@@ -4,6 +4,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <stdexcept>
@@ -80,6 +82,63 @@ struct DBuf {
     }
     return *this;
   }
+};
+
+// Page-locked host staging vector owned by the handle: host tables built per
+// solve (launch plans, offsets) are written here and copied to the device
+// asynchronously.  A copy from pageable memory may wait for the stream's
+// earlier work before it returns, which kept the host from planning while the
+// GPU ran; from page-locked memory the copy returns at once.  `upload`
+// records an event after the copy and `begin` waits for it, so the contents
+// are never rewritten under a pending copy.  Grows only (by doubling, keeping
+// the contents); freeing page-locked memory synchronises the device, so
+// growth should be rare.
+template <typename T>
+struct PinVec {
+  T* p = nullptr;
+  size_t len = 0, cap = 0;
+  cudaEvent_t done = nullptr;
+  void begin() {
+    if (done) cudaEventSynchronize(done);
+    len = 0;
+  }
+  void grow(size_t need) {
+    const size_t nc = std::max<size_t>(std::max<size_t>(need, 2 * cap), 256);
+    T* q = nullptr;
+    TABI_CUDA(cudaMallocHost(&q, nc * sizeof(T)));
+    if (len) std::memcpy(q, p, len * sizeof(T));
+    if (p) cudaFreeHost(p);
+    p = q;
+    cap = nc;
+  }
+  void push(const T& v) {
+    if (__builtin_expect(len == cap, 0)) grow(len + 1);
+    p[len++] = v;
+  }
+  void assign(const T* src, size_t n) {
+    begin();
+    if (n > cap) grow(n);
+    if (n) std::memcpy(p, src, n * sizeof(T));
+    len = n;
+  }
+  // the contents to dst (grown to at least one element) on stream s
+  void upload(DBuf<T>& dst, cudaStream_t s) {
+    dst.alloc(std::max<size_t>(len, 1));
+    if (len)
+      TABI_CUDA(cudaMemcpyAsync(dst.p, p, sizeof(T) * len, cudaMemcpyHostToDevice, s));
+    if (!done) TABI_CUDA(cudaEventCreateWithFlags(&done, cudaEventDisableTiming));
+    TABI_CUDA(cudaEventRecord(done, s));
+  }
+  ~PinVec() {
+    if (done) {
+      cudaEventSynchronize(done);
+      cudaEventDestroy(done);
+    }
+    if (p) cudaFreeHost(p);
+  }
+  PinVec() = default;
+  PinVec(const PinVec&) = delete;
+  PinVec& operator=(const PinVec&) = delete;
 };
 
 // Work item of the interaction kernels: node and a chunk of its entry list.
@@ -257,6 +316,13 @@ struct Handle {
   cudaStream_t stream = nullptr;
   cudaStream_t side = nullptr;           // second stream of the matvec (near field)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  // Streams of the leaf LU, forked from the caller's stream and joined back:
+  // the large-block group's chain at the highest priority, the trailing
+  // updates' columns beyond the next outer block (throughput work beside the
+  // chain) below it, and the small-block group at the lowest, so that the
+  // block scheduler gives freed SMs to the chain first.
+  cudaStream_t lu_hi = nullptr, lu_small = nullptr, aux = nullptr;
+  cudaEvent_t ev_la = nullptr, ev_rest = nullptr, ev_lu_join = nullptr;
   int device = 0;
   int n = 0;  // faces
   bool has_surface = false, has_tree = false, has_precond = false;
@@ -314,7 +380,13 @@ struct Handle {
     DBuf<int> dleaves;
     DBuf<int4> pitems, gitems;
     DBuf<double> scr;
+    PinVec<int> h_dleaves;  // page-locked staging of the three item lists
+    PinVec<int4> h_pitems, h_gitems;
   } pc_np[2];
+  // page-locked staging of the per-tree preconditioner tables
+  PinVec<int2> pc_h_tiles, pc_h_rng;
+  PinVec<int64_t> pc_h_blk_off, pc_h_dinv_off;
+  PinVec<int> pc_h_solve_list;
   DBuf<int> pc_fail, pc_big;
   DBuf<int2> pc_tiles2;
   int pc_pv_leaves = 0;  // leaves of the last tree factored with pivoting
@@ -392,6 +464,40 @@ inline void raise_smem_limit(const void* func, size_t bytes) {
   if (bytes <= h) return;
   TABI_CUDA(cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes));
   h = bytes;
+}
+
+// Programmatic dependent launch for chains of dependent kernels on one stream
+// (the leaf LU's diagonal, panel and update launches).  A kernel launched by
+// launch_chained may be scheduled while the kernel before it in the stream is
+// still running, once every CTA of that kernel has started and signalled
+// (chain_signal); it must call chain_wait before it reads anything the
+// earlier kernel writes.  chain_wait blocks until the earlier grid has
+// completed and its memory operations are visible, so the launch latency
+// between the two kernels overlaps the earlier one's tail.  In a kernel
+// launched the ordinary way, or after a non-kernel operation in the stream,
+// both are no-ops.
+__device__ __forceinline__ void chain_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+__device__ __forceinline__ void chain_signal() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// `chain` false launches the ordinary way: used for the first kernel after a
+// copy, an event record or a wait on another stream, so that such an
+// operation is never overtaken.
+template <typename... KArgs, typename... Args>
+void launch_chained(bool chain, void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                    cudaStream_t s, Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = chain ? 1 : 0;
+  TABI_CUDA(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
 }
 
 }  // namespace tabi
