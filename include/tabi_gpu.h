@@ -257,9 +257,27 @@ int tabi_direct_targets(tabi_h h, int nt, const int* targets, const double* x, d
  * far and near interactions and the leaf blocks of other targets are not
  * computed (the cluster moments still are: every shard needs all of them).
  * The shards' slices then assemble the full vector (an all-gather), and the
- * solve runs across shards; tabi_solve on a restricted handle is refused.
- * (0, nface) lifts the restriction. */
+ * solve runs across shards: tabi_solve / tabi_solve_dev on a restricted
+ * handle need an exchange (tabi_set_exchange) and are refused
+ * (TABI_ERR_STATE) without one.  (0, nface) lifts the restriction. */
 int tabi_set_target_range(tabi_h h, int t0, int t1);
+
+/* The exchange of a target-sharded solve (one handle per rank, each restricted
+ * by tabi_set_target_range to its own leaf-aligned range): after every
+ * operator and preconditioner application inside tabi_solve /
+ * tabi_solve_dev, the library calls fn(user, v_dev, n2, t0, t1, stream) with
+ * the device vector v_dev (n2 = 2 nface doubles) whose entries [t0, t1) and
+ * [nface + t0, nface + t1) this rank has just computed, and the stream the
+ * solve runs on; fn completes v_dev in place with the other ranks' slices
+ * (an all-gather, ordered on that stream) and returns 0, or non-zero on
+ * failure (the solve then fails with TABI_ERR_STATE).  Every rank then runs
+ * the same GMRES on identical vectors, so all ranks take the same steps and
+ * end with the same solution, which equals the unsharded solve's.  The
+ * reference has no counterpart (its solve is one process, main.f90:87-124);
+ * this replaces tabipb.sharded's host-side GMRES.  fn NULL removes it. */
+typedef int (*tabi_exchange_fn)(void* user, double* v_dev, int n2, int t0, int t1,
+                                void* stream);
+int tabi_set_exchange(tabi_h h, tabi_exchange_fn fn, void* user);
 
 /* main.f90:226-326 output_potential, after tabi_build_tree: x (2 nface) is
  * the solution in tree order as tabi_solve returns it; x_orig receives it in

@@ -163,6 +163,28 @@ void givens(double t1, double t2, double& c, double& s) {
   }
 }
 
+// A target-restricted handle computes its own shard of each operator and
+// preconditioner result; the exchange completes the vector with the other
+// ranks' slices (in place, ordered on s) before GMRES uses it.
+void shard_exchange(Handle& H, double* v, cudaStream_t s) {
+  if (!H.tree.ranged) return;
+  TABI_REQUIRE(H.xchg != nullptr, TABI_ERR_STATE, "a target range is set but no exchange");
+  const int rc = H.xchg(H.xchg_user, v, 2 * H.n, H.tree.rt0, H.tree.rt1, s);
+  TABI_REQUIRE(rc == 0, TABI_ERR_STATE,
+               "the shard exchange failed (tabi_set_exchange callback returned " +
+                   std::to_string(rc) + ")");
+}
+
+void op_matvec(Handle& H, const double* x, double* y, cudaStream_t s, bool shortcut) {
+  matvec_dev(H, x, y, s, shortcut);
+  shard_exchange(H, y, s);
+}
+
+void op_msolve(Handle& H, const double* r, double* z, cudaStream_t s) {
+  msolve_dev(H, r, z, s);
+  shard_exchange(H, z, s);
+}
+
 }  // namespace
 
 void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err_out,
@@ -230,7 +252,7 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
     TABI_CUDA(cudaMemcpyAsync(r, minv_b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     bnrm = minv_b_nrm;
   } else {
-    msolve_dev(H, b, r, s);
+    op_msolve(H, b, r, s);
     bnrm = nrm2_dev(H, r, n, s);
   }
   // the reference would iterate on NaNs to the iteration limit; a non-finite
@@ -246,7 +268,7 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
     if (ax < 1e-10)
       TABI_CUDA(cudaMemcpyAsync(r, x, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     else
-      matvec_dev(H, x, r, s, false);
+      op_matvec(H, x, r, s, false);
     { TABI_K(K_VEC, s); sub_kernel<<<vb, vt, 0, s>>>(n, b, r); }
   }
   for (;;) {
@@ -260,7 +282,7 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
     double snormw = 0.0, prod = 1.0, rho = 0.0;
     if (nrsts == 0 && !x_zero) {
       TABI_CUDA(cudaMemcpyAsync(wk, r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
-      msolve_dev(H, wk, r, s);
+      op_msolve(H, wk, r, s);
     }
     TABI_CUDA(cudaMemcpyAsync(Vc(1), r, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     double r0nrm = nrm2_dev(H, Vc(1), n, s);
@@ -276,8 +298,8 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
       for (int ll = 1; ll <= maxl; ++ll) {
         lgmr = ll;
         double* vn = Vc(ll + 1);
-        matvec_dev(H, Vc(ll), wk, s, false);  // |V(:,ll)| = 1: never the zero shortcut
-        msolve_dev(H, wk, vn, s);
+        op_matvec(H, Vc(ll), wk, s, false);  // |V(:,ll)| = 1: never the zero shortcut
+        op_msolve(H, wk, vn, s);
         // ---- DORTH: one cooperative launch for the whole sweep
         int i0 = std::max(1, ll - kmp + 1);
         {
@@ -427,9 +449,9 @@ void gmres_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
 // which also bounds the inner iterations in total).
 void solve_dev(Handle& H, const double* b, double* x, int* iter_out, double* err_out,
                int* ierr_out, double* hist, int* nhist, cudaStream_t s) {
-  TABI_REQUIRE(!H.tree.ranged, TABI_ERR_STATE,
-               "a target range is set: the handle computes one shard of the operator, the "
-               "solve runs across the shards (tabipb.sharded)");
+  TABI_REQUIRE(!H.tree.ranged || H.xchg, TABI_ERR_STATE,
+               "a target range is set: the handle computes one shard of the operator, and "
+               "the solve across the shards needs an exchange (tabi_set_exchange)");
   if (H.prm.precision != TABI_PREC_MIXED) {
     H.mv_prec = TABI_PREC_FP64;
     gmres_dev(H, b, x, iter_out, err_out, ierr_out, hist, nhist, s);
@@ -448,7 +470,7 @@ void solve_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
   double* d = H.d_ir_d.p;
   double* t = H.d_ir_t.p;
   const int vb = kVecBlocks, vt = 256;
-  msolve_dev(H, b, t, s);
+  op_msolve(H, b, t, s);
   const double bnrm = nrm2_dev(H, t, n, s);
   TABI_REQUIRE(std::isfinite(bnrm), TABI_ERR_ARG,
                "the right-hand side is not finite (|M^-1 b| is NaN or Inf)");
@@ -464,9 +486,9 @@ void solve_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
     if (outer == 0 && asum_dev(H, x, n, s) == 0.0) {
       TABI_CUDA(cudaMemcpyAsync(r, b, sizeof(double) * n, cudaMemcpyDeviceToDevice, s));
     } else {
-      matvec_dev(H, x, r, s, true);
+      op_matvec(H, x, r, s, true);
       { TABI_K(K_VEC, s); sub_kernel<<<vb, vt, 0, s>>>(n, b, r); }
-      msolve_dev(H, r, t, s);
+      op_msolve(H, r, t, s);
       tnrm = nrm2_dev(H, t, n, s);
     }
     err = tnrm / bnrm;
@@ -494,9 +516,9 @@ void solve_dev(Handle& H, const double* b, double* x, int* iter_out, double* err
     { TABI_K(K_VEC, s); axpy_kernel<<<vb, vt, 0, s>>>(n, 1.0, d, x); }
     if (ie == 2 || ie < 0) {  // stagnation (or an input error) of the inner solve
       H.mv_prec = TABI_PREC_FP64;
-      matvec_dev(H, x, r, s, true);
+      op_matvec(H, x, r, s, true);
       { TABI_K(K_VEC, s); sub_kernel<<<vb, vt, 0, s>>>(n, b, r); }
-      msolve_dev(H, r, t, s);
+      op_msolve(H, r, t, s);
       err = nrm2_dev(H, t, n, s) / bnrm;
       ierr = err <= tol ? 0 : ie;
       break;

@@ -376,13 +376,13 @@ int tabi_create(tabi_h* h, const tabi_params* p) {
     TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_join, cudaEventDisableTiming));
     int prio_lo = 0, prio_hi = 0;
     TABI_CUDA(cudaDeviceGetStreamPriorityRange(&prio_lo, &prio_hi));
-    // the large-block chain first, then the trailing updates beside it (the
-    // chain waits for them one outer block later), then the small-block group
-    // (a short chain of its own that ends long before the large one)
+    // the large-block chain first; the trailing updates beside it (the chain
+    // waits for them one outer block later) and the small-block group (a
+    // shorter chain of its own) share the SMs the chain leaves free
+    const int prio_mid = (prio_lo + prio_hi) / 2;
     TABI_CUDA(cudaStreamCreateWithPriority(&nh->H.lu_hi, cudaStreamNonBlocking, prio_hi));
-    TABI_CUDA(cudaStreamCreateWithPriority(&nh->H.aux, cudaStreamNonBlocking,
-                                           (prio_lo + prio_hi) / 2));
-    TABI_CUDA(cudaStreamCreateWithPriority(&nh->H.lu_small, cudaStreamNonBlocking, prio_lo));
+    TABI_CUDA(cudaStreamCreateWithPriority(&nh->H.aux, cudaStreamNonBlocking, prio_mid));
+    TABI_CUDA(cudaStreamCreateWithPriority(&nh->H.lu_small, cudaStreamNonBlocking, prio_mid));
     TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_la, cudaEventDisableTiming));
     TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_rest, cudaEventDisableTiming));
     TABI_CUDA(cudaEventCreateWithFlags(&nh->H.ev_lu_join, cudaEventDisableTiming));
@@ -817,6 +817,14 @@ int tabi_direct_targets(tabi_h h, int nt, const int* targets, const double* x, d
 }
 
 // ---- shards of the operator
+int tabi_set_exchange(tabi_h h, tabi_exchange_fn fn, void* user) {
+  if (!h) return TABI_ERR_ARG;
+  return guarded(h, [&] {
+    h->H.xchg = fn;
+    h->H.xchg_user = fn ? user : nullptr;
+  });
+}
+
 int tabi_set_target_range(tabi_h h, int t0, int t1) {
   if (!h) return TABI_ERR_ARG;
   return guarded(h, [&] {

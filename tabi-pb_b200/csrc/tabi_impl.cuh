@@ -317,11 +317,14 @@ struct Handle {
   cudaStream_t side = nullptr;           // second stream of the matvec (near field)
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // Streams of the leaf LU, forked from the caller's stream and joined back:
-  // the large-block group's chain at the highest priority, the trailing
+  // the large-block group's chain at the highest priority; the trailing
   // updates' columns beyond the next outer block (throughput work beside the
-  // chain) below it, and the small-block group at the lowest, so that the
-  // block scheduler gives freed SMs to the chain first.
+  // chain) and the small-block group below it, so that the block scheduler
+  // gives freed SMs to the chain first.
   cudaStream_t lu_hi = nullptr, lu_small = nullptr, aux = nullptr;
+  // the exchange of a target-sharded solve (tabi_set_exchange)
+  tabi_exchange_fn xchg = nullptr;
+  void* xchg_user = nullptr;
   cudaEvent_t ev_la = nullptr, ev_rest = nullptr, ev_lu_join = nullptr;
   int device = 0;
   int n = 0;  // faces

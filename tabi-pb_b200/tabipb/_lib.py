@@ -35,8 +35,12 @@ SYMBOLS = [
     "tabi_ws_train_step_dev", "tabi_ws_graph_dev", "tabi_set_warmstart", "tabi_batch_run_dev",
     "tabi_output_potential", "tabi_output_potential_dev", "tabi_set_target_range",
     "tabi_direct_targets", "tabi_pivoted_leaves", "tabi_probe_fp32_peak",
-    "tabi_face_filter_dev",
+    "tabi_face_filter_dev", "tabi_set_exchange",
 ]
+
+# tabi_exchange_fn: int (*)(void* user, double* v_dev, int n2, int t0, int t1, void* stream)
+EXCHANGE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_int, C.c_int, C.c_int,
+                          C.c_void_p)
 
 
 PREC_FP64 = 0   # TABI_PREC_FP64: the reference's FP64 arithmetic
@@ -131,6 +135,7 @@ def load(path: str = LIB_PATH):
     L.tabi_ws_graph_dev.argtypes = [_vp, C.c_int, _vp, _vp, _vp, _vp, _vp, _ip, _fp, _vp]
     L.tabi_set_warmstart.argtypes = [_vp, _vp]
     L.tabi_set_target_range.argtypes = [_vp, C.c_int, C.c_int]
+    L.tabi_set_exchange.argtypes = [_vp, EXCHANGE_FN, _vp]
     L.tabi_direct_targets.argtypes = [_vp, C.c_int, _ip, _dp, _dp]
     L.tabi_pivoted_leaves.argtypes = [_vp, _ip]
     L.tabi_output_potential.argtypes = [_vp, C.c_int, _dp, C.c_int, _ip, _dp, _dp, _dp]

@@ -13,6 +13,14 @@ single-GPU solve), so every rank takes the same steps and ends with the same
 solution.
 
 The exchange uses torch.distributed: NCCL between GPUs, gloo on the host.
+
+Two drivers share that exchange.  `sharded_solve` runs the library's own
+GMRES (tabi_solve) on every rank: the handle calls back after each operator
+and preconditioner application (tabi_set_exchange) and `DeviceExchange`
+completes the device vector in place on the library's stream, so the
+vectors never leave the GPU with NCCL (gloo, a host backend, stages the
+slices through host memory).  `ShardedOperator` + `dgmres` keep the
+host-side form, which the CPU tests drive with the oracle's operator.
 """
 from __future__ import annotations
 
@@ -229,3 +237,100 @@ def dgmres(matvec, msolve, b, x0=None, tol=1e-4, maxl=10, nrmax=10):
         ierr = 2
         break
     return dict(x=x, iter=it, err=err, ierr=ierr, err_hist=np.asarray(hist))
+
+
+def _slice_index(bounds):
+    """(width, index): the all-gather buffer holds rank r's slices at
+    [r * 2 width, r * 2 width + t1 - t0) and [r * 2 width + width, ...); index
+    maps every entry of the full 2n vector to its place in that buffer."""
+    b = np.asarray(bounds, np.int64)
+    n = int(b[-1])
+    width = int(np.max(np.diff(b)))
+    idx = np.empty(2 * n, np.int64)
+    for r in range(len(b) - 1):
+        a0, a1 = int(b[r]), int(b[r + 1])
+        base = r * 2 * width
+        idx[a0:a1] = base + np.arange(a1 - a0)
+        idx[n + a0:n + a1] = base + width + np.arange(a1 - a0)
+    return width, idx
+
+
+def exchange_slices(v, bounds, rank, group=None, index=None):
+    """Completes v (a torch tensor of 2n, on the host or the GPU) in place
+    with every rank's slices [t0, t1) and [n + t0, n + t1) of the tree order:
+    one all-gather of this rank's two slices, then one gather into v.  A CUDA
+    tensor stays on the device with NCCL; gloo stages it through the host."""
+    import torch
+    import torch.distributed as dist
+
+    b = np.asarray(bounds, np.int64)
+    n = int(b[-1])
+    width, idx = index if index is not None else _slice_index(b)
+    t0, t1 = int(b[rank]), int(b[rank + 1])
+    mine = torch.zeros(2 * width, dtype=v.dtype, device=v.device)
+    mine[: t1 - t0] = v[t0:t1]
+    mine[width:width + t1 - t0] = v[n + t0:n + t1]
+    host = v.is_cuda and dist.get_backend(group) != "nccl"
+    src = mine.cpu() if host else mine
+    parts = [torch.empty_like(src) for _ in range(len(b) - 1)]
+    dist.all_gather(parts, src, group=group)
+    flat = torch.cat(parts).to(v.device)
+    if not torch.is_tensor(idx):
+        idx = torch.as_tensor(idx, device=v.device)
+    v.copy_(flat[idx])
+
+
+class _DevVec:
+    """A raw device pointer of n doubles as a zero-copy torch tensor
+    (__cuda_array_interface__)."""
+
+    def __init__(self, ptr, n):
+        self.__cuda_array_interface__ = {"shape": (int(n),), "typestr": "<f8",
+                                         "data": (int(ptr), False), "version": 3,
+                                         "strides": None}
+
+
+class DeviceExchange:
+    """The tabi_set_exchange callback of one rank: completes the library's
+    device vector on the library's stream (exchange_slices)."""
+
+    def __init__(self, bounds, rank, group=None, device=None):
+        import torch
+
+        self.bounds = np.asarray(bounds, np.int64)
+        self.rank = rank
+        self.group = group
+        self.device = torch.device(device if device is not None else "cuda")
+        width, idx = _slice_index(self.bounds)
+        self.index = (width, torch.as_tensor(idx, device=self.device))
+        self.calls = 0
+
+    def __call__(self, v_ptr, n2, t0, t1, stream):
+        import torch
+
+        assert n2 == 2 * int(self.bounds[-1])
+        assert (t0, t1) == (int(self.bounds[self.rank]), int(self.bounds[self.rank + 1]))
+        self.calls += 1
+        with torch.cuda.stream(torch.cuda.ExternalStream(int(stream or 0), device=self.device)):
+            v = torch.as_tensor(_DevVec(v_ptr, n2), device=self.device)
+            exchange_slices(v, self.bounds, self.rank, self.group, self.index)
+
+
+def sharded_solve(solver, b, bounds, rank, group=None, device=None):
+    """The library's solve (tabi_solve: DGMRES, or GMRES-IR in mixed
+    precision) across ranks: this rank's handle restricted to its shard, the
+    exchange completing every operator and preconditioner result.  Every rank
+    returns the same result, equal to the unsharded solve's."""
+    solver.set_target_range(int(bounds[rank]), int(bounds[rank + 1]))
+    ex = DeviceExchange(bounds, rank, group, device)
+    solver.set_exchange(ex)
+    try:
+        res = solver.dgmres(b)
+    except Exception:
+        if getattr(solver, "exchange_error", None) is not None:
+            raise solver.exchange_error
+        raise
+    finally:
+        solver.set_exchange(None)
+    res["exchanges"] = ex.calls
+    return res

@@ -213,6 +213,28 @@ class TabiSolver:
         (leaf-aligned): only that slice of y / z is written."""
         check(self.h, self.L.tabi_set_target_range(self.h, int(t0), int(t1)))
 
+    def set_exchange(self, fn):
+        """The exchange of a target-sharded solve (tabi_set_exchange):
+        fn(v_dev_ptr, n2, t0, t1, stream_ptr) completes the device vector in
+        place with the other ranks' slices and returns None, or raises.  None
+        removes it.  The ctypes callback is kept alive by the solver."""
+        if fn is None:
+            self._xchg = None
+            check(self.h, self.L.tabi_set_exchange(self.h, _lib.EXCHANGE_FN(), None))
+            return
+
+        def cb(user, v, n2, t0, t1, stream):
+            try:
+                fn(v, n2, t0, t1, stream)
+                return 0
+            except Exception as e:  # noqa: BLE001 -- reported through the return code
+                self.exchange_error = e
+                return 1
+
+        self._xchg = _lib.EXCHANGE_FN(cb)
+        self.exchange_error = None
+        check(self.h, self.L.tabi_set_exchange(self.h, self._xchg, None))
+
     # ---- main.f90:226-326
     def output_potential(self, sptpos, nvert, x):
         """x (tree order, as dgmres returns it) -> (x in the original face order

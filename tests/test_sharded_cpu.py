@@ -115,3 +115,49 @@ def test_shard_bounds_are_leaf_aligned_and_balanced():
         ends = set((starts + sizes).tolist()) | {0}
         assert all(int(v) in ends for v in b)
         assert np.diff(b).max() <= sizes.sum() / k + sizes.max()
+
+
+def _exchange_rank(rank, world, port, outdir, bounds):
+    import sys
+
+    here = os.path.dirname(os.path.abspath(__file__))
+    root = os.path.dirname(here)
+    sys.path[:0] = [here, os.path.join(root, "tabi-pb_b200")]
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    from tabipb import sharded as SH
+
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        b = np.asarray(bounds)
+        n = int(b[-1])
+        full = torch.arange(2 * n, dtype=torch.float64) * 0.5 + 1.0
+        # this rank knows its own slices only; the rest is garbage
+        v = torch.full((2 * n,), float("nan"), dtype=torch.float64)
+        t0, t1 = int(b[rank]), int(b[rank + 1])
+        v[t0:t1] = full[t0:t1]
+        v[n + t0:n + t1] = full[n + t0:n + t1]
+        SH.exchange_slices(v, b, rank)
+        np.save(os.path.join(outdir, f"ex{rank}.npy"), v.numpy())
+        np.save(os.path.join(outdir, "full.npy"), full.numpy())
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("bounds", [[0, 3, 7], [0, 5, 5, 9], [0, 1, 11, 12]])
+def test_exchange_completes_every_rank(tmp_path, bounds):
+    """exchange_slices (the all-gather of tabi_set_exchange's callback):
+    uneven and empty shards, every rank ends with the whole vector."""
+    import torch.multiprocessing as mp
+
+    world = len(bounds) - 1
+    mp.start_processes(_exchange_rank, args=(world, _free_port(), str(tmp_path), bounds),
+                       nprocs=world, join=True, start_method="spawn")
+    full = np.load(tmp_path / "full.npy")
+    for r in range(world):
+        np.testing.assert_array_equal(np.load(tmp_path / f"ex{r}.npy"), full)
