@@ -1267,24 +1267,19 @@ constexpr size_t kNPPanelSmem = sizeof(double) * 2 * kNP * kNPPitch;
 
 // Per leaf (leaves[blockIdx.x]) with m > k0: D = A[k0:k0+d, k0:k0+d], d =
 // min(64, m - k0), factored in place without interchanges (DGETRF2's scaling:
-// reciprocal unless the pivot is below the smallest normal; the rank-1 updates
-// on a 16 x 16 thread grid); scr receives L^{-1} (unit lower, column-major)
-// and U^{-1} (row-major) of D, 64 x 64 each with zeros outside the triangle,
-// and dinv the 32 x 32 diagonal blocks of both (identity padded, the layout
-// lu_diaginv_kernel writes).  The inverses go by 32 x 32 blocks: four warps
-// invert the diagonal blocks of L and U (one column per lane, unrolled), then
-// L^{-1}_21 = -L22^{-1} (L21 L11^{-1}) and U^{-1}_12 = -U11^{-1} (U12 U22^{-1})
-// by two small products through the zero blocks of the result as scratch.
+// multipliers times the pivot's reciprocal); scr receives L^{-1} (unit lower,
+// column-major) and U^{-1} (row-major) of D, 64 x 64 each with zeros outside
+// the triangle and from d on, and dinv the 32 x 32 diagonal blocks of both
+// (identity padded, the layout lu_diaginv_kernel writes).  The block, L^{-1}
+// and U^{-1} live in registers on a 16 x 16 thread grid; one loop of d
+// steps with one barrier each factors the block and forms both inverses
+// (the loop's comment gives the scheme).  Every entry of the factors takes
+// the same sequence of updates as in a column-by-column DGETF2 order.
 // one double into shared memory, asynchronously (zero when !valid)
 __device__ __forceinline__ void cp_async8(double* dst, const double* src, bool valid) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
                "r"(valid ? 8 : 0));
-}
-
-__device__ __forceinline__ double np_entry(const double (*D)[kNPPitch], int o, int nb, int i,
-                                           int q) {
-  return (i < nb && q < nb) ? D[o + i][o + q] : (i == q ? 1.0 : 0.0);
 }
 
 __global__ void __launch_bounds__(kNPT) lu_np_diag_kernel(
@@ -1302,217 +1297,137 @@ __global__ void __launch_bounds__(kNPT) lu_np_diag_kernel(
   const int m = 2 * leaf_rng[leaf].y;
   const int d = min(kNP, m - k0);
   double* A = lu + blk_off[leaf];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int tid = threadIdx.x;
   for (int e = tid; e < kNP * kNP; e += kNPT) {
     const int c = e >> 6, r = e & 63;
     cp_async8(&D[r][c], A + (size_t)(k0 + min(c, d - 1)) * m + k0 + min(r, d - 1),
               r < d && c < d);
   }
   asm volatile("cp.async.commit_group;\n" ::);
-  for (int e = tid; e < kNP * kNPPitch; e += kNPT) {
-    (&Li[0][0])[e] = 0.0;
-    (&Ui[0][0])[e] = 0.0;
-  }
   __shared__ double s_rcp[kNP];  // reciprocal of each pivot
+  __shared__ double s_row[2][kNP], s_col[2][kNP], s_xrow[2][kNP], s_zcol[2][kNP];
   asm volatile("cp.async.wait_group 0;\n" ::);
   __syncthreads();
-  // 2 x 2 blocks of 32: LU(D11) by warp 0 in registers; U12 = L11^{-1} D12
-  // (warp 1) and L21 = D21 U11^{-1} (warp 2); D22 -= L21 U12 (all warps);
-  // LU(D22) by warp 0.  DGETRF2's scaling throughout: a multiplier is the
-  // updated entry times the pivot's reciprocal (divided when the pivot is
-  // below the smallest normal).
+  // Thread (tx, ty) of a 16 x 16 grid holds rows ty + 16p and columns
+  // tx + 16q (p, q < 4) of the block in registers, and of X = L^{-1} and
+  // Z = U^{-1}.  The column loop runs as four rolled loops of 16 (one per
+  // band jp), so every register index and every band range is a compile-time
+  // constant; a short rolled loop also keeps the code that this
+  // once-per-launch kernel fetches small.  Entries of finished rows and
+  // columns within a band take a zero multiplier or row entry, which leaves
+  // them unchanged, so the updates need no predicates.
+  //
+  // Step j, one barrier (published vectors double-buffered by parity):
+  //  * the factorisation (DGETRF2's scaling): row j and column j, unscaled,
+  //    are published; every thread forms its rows' multipliers with the
+  //    pivot's reciprocal and updates its entries right of and below the
+  //    pivot.  The reciprocal of pivot j + 1 is formed during step j by the
+  //    thread that holds that entry, right after its update, and stored for
+  //    step j + 1.  A pivot that is zero, subnormal (where DGETRF2 divides
+  //    instead) or not finite fails the certificate, and the leaf goes to
+  //    the pivoted kernels, which follow DGETRF2 there.
+  //  * X by forward row operations, row i -= L[i][j] (row j of X), with row j
+  //    final at step j and L[i][j] the step's multiplier;
+  //  * Z by column operations, column j times the pivot's reciprocal, then
+  //    column c -= U[j][c] (column j of Z), with U[j][c] the step's row.
+  // X is lower and Z upper triangular, so step j changes X in rows of bands
+  // >= jp and columns of bands <= jp, Z the other way round.
+  const int tx = tid & 15, ty = tid >> 4;
   bool bad = false;
-  const int n2 = max(0, d - kDB);
-  for (int blk = 0; blk < 2; ++blk) {
-    const int o = blk * kDB, nb = blk == 0 ? min(kDB, d) : n2;
-    if (nb > 0 && warp == 0) {
-      const int r = lane;  // this lane's row of the block
-      double a[kDB];
+  double a[4][4], x[4][4], z[4][4];
 #pragma unroll
-      for (int c = 0; c < kDB; ++c) a[c] = (r < nb && c < nb) ? D[o + r][o + c] : 0.0;
+  for (int p = 0; p < 4; ++p)
 #pragma unroll
-      for (int j = 0; j < kDB; ++j) {
-        if (j < nb) {
-          const double pk = __shfl_sync(0xffffffffu, a[j], j);
-          if (!(pk != 0.0 && isfinite(pk))) bad = true;
-          const bool recip = fabs(pk) >= 2.2250738585072014e-308;
-          const double rcp = 1.0 / pk;
-          if (lane == 0) s_rcp[o + j] = recip ? rcp : 0.0;
-          const double l = recip ? a[j] * rcp : a[j] / pk;
-          if (r > j && r < nb) {
-            if (!(fabs(l) <= kNoPivBound)) bad = true;
-            a[j] = l;
+    for (int q = 0; q < 4; ++q) {
+      const int i = ty + 16 * p, c = tx + 16 * q;
+      a[p][q] = D[i][c];
+      x[p][q] = z[p][q] = (i == c && i < d) ? 1.0 : 0.0;
+    }
+  auto pivot_rcp = [&](int j, double pk) {  // by the holder of entry (j, j)
+    if (!(fabs(pk) >= 2.2250738585072014e-308 && fabs(pk) <= 1.7976931348623157e308)) bad = true;
+    s_rcp[j] = 1.0 / pk;
+  };
+  if (tid == 0) pivot_rcp(0, a[0][0]);
+#pragma unroll
+  for (int jp = 0; jp < 4; ++jp) {
+#pragma unroll 1
+    for (int jt = 0; jt < 16; ++jt) {
+      const int j = 16 * jp + jt, b = j & 1;
+      if (j >= d) break;
+      if (ty == jt) {
+#pragma unroll
+        for (int q = jp; q < 4; ++q) s_row[b][tx + 16 * q] = a[jp][q];
+#pragma unroll
+        for (int q = 0; q <= jp; ++q) s_xrow[b][tx + 16 * q] = x[jp][q];
+      }
+      if (tx == jt) {
+#pragma unroll
+        for (int p = jp; p < 4; ++p) s_col[b][ty + 16 * p] = a[p][jp];
+#pragma unroll
+        for (int p = 0; p <= jp; ++p) s_zcol[b][ty + 16 * p] = z[p][jp];
+      }
+      __syncthreads();
+      const double rcp = s_rcp[j];
+      double l[4], u[4], ux[4], zc[4];
+#pragma unroll
+      for (int p = jp; p < 4; ++p) {
+        const int i = ty + 16 * p;
+        l[p] = i > j ? s_col[b][i] * rcp : 0.0;
+      }
+#pragma unroll
+      for (int q = jp; q < 4; ++q) {
+        const int c = tx + 16 * q;
+        u[q] = c > j ? s_row[b][c] : 0.0;
+      }
+#pragma unroll
+      for (int q = 0; q <= jp; ++q) ux[q] = s_xrow[b][tx + 16 * q];
+#pragma unroll
+      for (int p = 0; p <= jp; ++p) zc[p] = s_zcol[b][ty + 16 * p] * rcp;
+      if (tx == jt) {  // the holders of column j: its multipliers, column j of Z scaled
+#pragma unroll
+        for (int p = jp; p < 4; ++p)
+          if (ty + 16 * p > j) {
+            if (!(fabs(l[p]) <= kNoPivBound)) bad = true;
+            a[p][jp] = l[p];
           }
 #pragma unroll
-          for (int c = j + 1; c < kDB; ++c) {
-            const double u = __shfl_sync(0xffffffffu, a[c], j);
-            if (r > j && r < nb) a[c] = fma(-l, u, a[c]);
-          }
-        }
+        for (int p = 0; p <= jp; ++p) z[p][jp] = zc[p];
       }
-      if (r < nb)
 #pragma unroll
-        for (int c = 0; c < kDB; ++c)
-          if (c < nb) D[o + r][o + c] = a[c];
+      for (int p = jp; p < 4; ++p)
+#pragma unroll
+        for (int q = jp; q < 4; ++q) a[p][q] = fma(-l[p], u[q], a[p][q]);
+      // the next pivot's reciprocal, by its holder
+      if (tx == ty && tx == ((j + 1) & 15) && j + 1 < d) {
+        if (jt < 15)
+          pivot_rcp(j + 1, a[jp][jp]);
+        else if (jp < 3)
+          pivot_rcp(j + 1, a[jp < 3 ? jp + 1 : 3][jp < 3 ? jp + 1 : 3]);
+      }
+#pragma unroll
+      for (int p = jp; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q <= jp; ++q) x[p][q] = fma(-l[p], ux[q], x[p][q]);
+#pragma unroll
+      for (int p = 0; p <= jp; ++p)
+#pragma unroll
+        for (int q = jp; q < 4; ++q) z[p][q] = fma(-zc[p], u[q], z[p][q]);
     }
-    __syncthreads();
-    if (blk == 1 || n2 == 0) break;
-    if (warp == 1 && lane < n2) {
-      // U12: column kDB + lane of the block row, forward substitution with L11
-      const int c = kDB + lane;
-      double x[kDB];
-#pragma unroll
-      for (int r = 0; r < kDB; ++r) {
-        double v = D[r][c];
-#pragma unroll
-        for (int q = 0; q < kDB; ++q)
-          if (q < r) v = fma(-D[r][q], x[q], v);
-        x[r] = v;
-      }
-#pragma unroll
-      for (int r = 0; r < kDB; ++r) D[r][c] = x[r];
-    } else if (warp == 2 && lane < n2) {
-      // L21: row kDB + lane, x U11 = D21 row, with the pivots' reciprocals
-      const int r = kDB + lane;
-      double x[kDB];
-#pragma unroll
-      for (int c = 0; c < kDB; ++c) {
-        double v = D[r][c];
-#pragma unroll
-        for (int q = 0; q < kDB; ++q)
-          if (q < c) v = fma(-x[q], D[q][c], v);
-        const double pk = D[c][c], rc = s_rcp[c];
-        v = rc != 0.0 ? v * rc : v / pk;
-        if (!(fabs(v) <= kNoPivBound)) bad = true;
-        x[c] = v;
-      }
-#pragma unroll
-      for (int c = 0; c < kDB; ++c) D[r][c] = x[c];
-    }
-    __syncthreads();
-    // D22 -= L21 U12: thread (row tid / 8, columns 4 (tid % 8) ..)
-    {
-      const int r = tid >> 3, c4 = (tid & 7) * 4;
-      if (r < n2) {
-        double acc[4];
-#pragma unroll
-        for (int b = 0; b < 4; ++b) acc[b] = D[kDB + r][kDB + c4 + b];
-#pragma unroll 8
-        for (int q = 0; q < kDB; ++q) {
-          const double l = D[kDB + r][q];
-#pragma unroll
-          for (int b = 0; b < 4; ++b) acc[b] = fma(-l, D[q][kDB + c4 + b], acc[b]);
-        }
-#pragma unroll
-        for (int b = 0; b < 4; ++b)
-          if (c4 + b < n2) D[kDB + r][kDB + c4 + b] = acc[b];
-      }
-    }
-    __syncthreads();
   }
+#pragma unroll
+  for (int p = 0; p < 4; ++p)
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      const int i = ty + 16 * p, c = tx + 16 * q;
+      D[i][c] = a[p][q];
+      Li[i][c] = x[p][q];
+      Ui[i][c] = z[p][q];
+    }
+  __syncthreads();
   // factors back
   for (int e = tid; e < d * d; e += kNPT) {
     const int c = e / d, r = e - c * d;
     A[(size_t)(k0 + c) * m + k0 + r] = D[r][c];
-  }
-  // inverses of the 32 x 32 diagonal blocks: warp 0/1 L (blocks 0/1), warp 2/3 U
-  if (warp < 4) {
-    const int b = warp & 1, o = b * kDB, nb = min(kDB, d - o);
-    if (nb > 0) {
-      double x[kDB];
-      if (warp < 2) {
-#pragma unroll
-        for (int i = 0; i < kDB; ++i) {
-          double v = (i == lane) ? 1.0 : 0.0;
-#pragma unroll
-          for (int q = 0; q < kDB; ++q)
-            if (q < i) v = fma(-np_entry(D, o, nb, i, q), x[q], v);
-          x[i] = v;
-        }
-        if (lane < nb)
-#pragma unroll
-          for (int i = 0; i < kDB; ++i)
-            if (i < nb) Li[o + i][o + lane] = x[i];
-      } else {
-#pragma unroll
-        for (int i = kDB - 1; i >= 0; --i) {
-          double v = (i == lane) ? 1.0 : 0.0;
-#pragma unroll
-          for (int q = 0; q < kDB; ++q)
-            if (q > i) v = fma(-np_entry(D, o, nb, i, q), x[q], v);
-          x[i] = v / np_entry(D, o, nb, i, i);
-        }
-        if (lane < nb)
-#pragma unroll
-          for (int i = 0; i < kDB; ++i)
-            if (i < nb) Ui[o + i][o + lane] = x[i];
-      }
-    }
-  }
-  __syncthreads();
-  if (d > kDB) {
-    const int n2 = d - kDB;  // order of the second diagonal block
-    // T = L21 L11^{-1} into Li's (zero) upper-right block, T' = U12 U22^{-1}
-    // into Ui's (zero) lower-left block
-    for (int e = tid; e < kDB * kDB; e += kNPT) {
-      const int r = e / kDB, c = e - r * kDB;
-      // full 32-term sums (the inverses are zero outside their triangles),
-      // two accumulators each
-      if (r < n2) {  // T[r][c], r < n2, c < 32
-        double v0 = 0.0, v1 = 0.0;
-#pragma unroll
-        for (int q = 0; q < kDB; q += 2) {
-          v0 = fma(D[kDB + r][q], Li[q][c], v0);
-          v1 = fma(D[kDB + r][q + 1], Li[q + 1][c], v1);
-        }
-        Li[c][kDB + r] = v0 + v1;  // stored transposed in the free block
-      }
-      if (c < n2) {  // T'[r][c], r < 32, c < n2
-        double v0 = 0.0, v1 = 0.0;
-#pragma unroll
-        for (int q = 0; q < kDB; q += 2) {
-          v0 = fma(D[r][kDB + q], Ui[kDB + q][kDB + c], v0);
-          v1 = fma(D[r][kDB + q + 1], Ui[kDB + q + 1][kDB + c], v1);
-        }
-        Ui[kDB + c][r] = v0 + v1;  // transposed
-      }
-    }
-    __syncthreads();
-    double l21[4], u12[4];
-    int nv = 0;
-    for (int e = tid; e < kDB * kDB; e += kNPT, ++nv) {
-      const int r = e / kDB, c = e - r * kDB;
-      double a = 0.0, bb = 0.0;
-      if (r < n2) {  // -(L22^{-1} T)[r][c]
-        double a1 = 0.0;
-#pragma unroll
-        for (int q = 0; q < kDB; q += 2) {
-          a = fma(Li[kDB + r][kDB + q], Li[c][kDB + q], a);
-          a1 = fma(Li[kDB + r][kDB + q + 1], Li[c][kDB + q + 1], a1);
-        }
-        a += a1;
-      }
-      if (c < n2) {  // -(U11^{-1} T')[r][c]
-        double b1 = 0.0;
-#pragma unroll
-        for (int q = 0; q < kDB; q += 2) {
-          bb = fma(Ui[r][q], Ui[kDB + c][q], bb);
-          b1 = fma(Ui[r][q + 1], Ui[kDB + c][q + 1], b1);
-        }
-        bb += b1;
-      }
-      l21[nv] = -a;
-      u12[nv] = -bb;
-    }
-    __syncthreads();
-    nv = 0;
-    for (int e = tid; e < kDB * kDB; e += kNPT, ++nv) {
-      const int r = e / kDB, c = e - r * kDB;
-      Li[c][kDB + r] = 0.0;
-      Ui[kDB + c][r] = 0.0;
-      if (r < n2) Li[kDB + r][c] = l21[nv];
-      if (c < n2) Ui[r][kDB + c] = u12[nv];
-    }
   }
   if (__syncthreads_or(bad) && tid == 0) fail[leaf] = 1;
   double* S = scr + (size_t)blockIdx.x * 2 * kNP * kNP;
