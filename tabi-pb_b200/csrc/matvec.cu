@@ -626,7 +626,7 @@ void set_target_range(Handle& H, int t0, int t1, cudaStream_t s) {
   TABI_REQUIRE(boundary(t0) && boundary(t1), TABI_ERR_ARG,
                "target range must start and end on leaf boundaries (tree order)");
   // the interaction entries of targets in range, item by item
-  auto restrict_list = [&](const std::vector<WorkItem>& work, const DBuf<int2>& ent,
+  auto restrict_list = [&](const PinVec<WorkItem>& work, const DBuf<int2>& ent,
                            std::vector<WorkItem>& rwork, DBuf<WorkItem>& d_rwork,
                            DBuf<int2>& d_rent) {
     size_t total = 0;

@@ -1700,7 +1700,7 @@ void build_precond(Handle& H, cudaStream_t s) {
   T.blk_off.resize(nl);
   int64_t off = 0;
   PinVec<int2>& tiles = H.pc_h_tiles;
-  tiles.begin();
+  tiles.restart();
   for (int l = 0; l < nl; ++l) {
     int c = T.leaves[l];
     rng[l] = make_int2(T.ibeg[c], T.num[c]);
@@ -1727,11 +1727,27 @@ void build_precond(Handle& H, cudaStream_t s) {
                                                     H.d_ny.p, H.d_nz.p, H.d_area.p,
                                                     H.prm.kappa, eps, T.d_lu.p); }
   TABI_CUDA(cudaMemsetAsync(d_info.p, 0, sizeof(int) * nl, s));
+  // apply lists (they depend on the leaf sizes only, so they are built while
+  // the assembly runs): blocks of order > 512 get 512 threads (one wave on the GPU),
+  // the others 256 threads on the side stream; largest first in each
+  {
+    std::vector<int> big, small;
+    for (int l = 0; l < nl; ++l) (2 * rng[l].y > 512 ? big : small).push_back(l);
+    std::sort(big.begin(), big.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
+    std::sort(small.begin(), small.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
+    T.n_solve_big = (int)big.size();
+    T.n_solve_small = (int)small.size();
+    big.insert(big.end(), small.begin(), small.end());
+    H.pc_h_solve_list.assign(big.data(), big.size());
+    H.pc_h_solve_list.upload(T.d_solve_list, s);
+  }
   // Two leaf groups with plans of their own: blocks of order above
-  // kLuSmallBlock on the handle's stream, the others on its side stream, so
-  // the many short factorisations of small leaves run beside the long chain of
-  // steps of the large ones instead of inside its launches; one fork after the
-  // assembly, one join at the end.
+  // kLuSmallBlock and the others, so the many short factorisations of small
+  // leaves run beside the long chain of steps of the large ones instead of
+  // inside its launches.  The unpivoted factorisation runs them on the
+  // handle's LU streams (see below); the pivoted one on the caller's stream
+  // and the side stream, with one fork after the assembly and one join at
+  // the end (fork / join).
   auto fork = [&](bool split) {
     if (!split) return;
     TABI_CUDA(cudaEventRecord(H.ev_fork, s));
@@ -1792,23 +1808,24 @@ void build_precond(Handle& H, cudaStream_t s) {
     // columns right of it (rows of the block, columns beyond) wait for the
     // auxiliary stream.  Every entry is updated by the same tile in the same
     // k order as without the split, so the factors are the same bit for bit.
-    auto run_np = [&](const std::vector<int>& order, Handle::NpPlan& B, cudaStream_t st,
-                      bool la) {
+    struct Launch {
+      // 0 diagonal, 1 panel, 2 update, 3 fork to the auxiliary stream,
+      // 4 wait for the auxiliary stream, 5 update on the auxiliary stream
+      int kind;
+      int k0, depth, off, cnt, scr_slot0;
+    };
+    // one group's plan: item lists (uploaded on st) and its launches
+    auto plan_np = [&](const std::vector<int>& order, Handle::NpPlan& B, cudaStream_t st,
+                       bool la) {
       int gmax = 0;
       for (int l : order) gmax = std::max(gmax, 2 * rng[l].y);
-      struct Launch {
-        // 0 diagonal, 1 panel, 2 update, 3 fork to the auxiliary stream,
-        // 4 wait for the auxiliary stream, 5 update on the auxiliary stream
-        int kind;
-        int k0, depth, off, cnt, scr_slot0;
-      };
       std::vector<Launch> plan;
       PinVec<int>& dl = B.h_dleaves;
       PinVec<int4>& pit = B.h_pitems;
       PinVec<int4>& git = B.h_gitems;
-      dl.begin();
-      pit.begin();
-      git.begin();
+      dl.restart();
+      pit.restart();
+      git.restart();
       const auto pack = [](int re, int ce) { return (re << 16) | ce; };
       int max_slots = 1;
       auto emit = [&](int kind, int k0, int depth, size_t before, size_t after, int slot0) {
@@ -1905,10 +1922,24 @@ void build_precond(Handle& H, cudaStream_t s) {
       pit.upload(B.pitems, st);
       git.upload(B.gitems, st);
       B.scr.alloc((size_t)max_slots * (kOB2 / kNP) * 2 * kNP * kNP);
-      // kernels follow kernels on `st` as a programmatic chain; the first one
-      // after the uploads or a cross-stream event starts the ordinary way
+      return plan;
+    };
+    // Issues launch `at` of a group's plan.  Kernels follow kernels on the
+    // group's stream as a programmatic chain; the first one after the uploads
+    // or a cross-stream event starts the ordinary way.
+    struct Issuer {
+      std::vector<Launch> plan;
+      Handle::NpPlan* B;
+      cudaStream_t st;
+      size_t at = 0;
       bool chain = false;
-      for (const Launch& q : plan) {
+    };
+    auto issue_one = [&](Issuer& is) {
+      const Launch& q = is.plan[is.at++];
+      Handle::NpPlan& B = *is.B;
+      cudaStream_t st = is.st;
+      bool& chain = is.chain;
+      {
         if (q.kind == 0) {
           TABI_K(K_LU, st);
           launch_chained(chain, lu_np_diag_kernel, dim3(q.cnt), dim3(kNPT), kNPDiagSmem, st,
@@ -1941,8 +1972,19 @@ void build_precond(Handle& H, cudaStream_t s) {
         }
       }
     };
-    if (!grp[0].empty()) run_np(grp[0], H.pc_np[0], H.lu_hi, true);
-    if (!grp[1].empty()) run_np(grp[1], H.pc_np[1], H.lu_small, false);
+    // both plans first, then their launches interleaved, so that both chains
+    // start at once (the host issues far faster than the GPU runs them)
+    Issuer big{}, small{};
+    big.B = &H.pc_np[0];
+    big.st = H.lu_hi;
+    small.B = &H.pc_np[1];
+    small.st = H.lu_small;
+    if (!grp[0].empty()) big.plan = plan_np(grp[0], H.pc_np[0], H.lu_hi, true);
+    if (!grp[1].empty()) small.plan = plan_np(grp[1], H.pc_np[1], H.lu_small, false);
+    while (big.at < big.plan.size() || small.at < small.plan.size()) {
+      if (big.at < big.plan.size()) issue_one(big);
+      if (small.at < small.plan.size()) issue_one(small);
+    }
     TABI_CUDA(cudaEventRecord(H.ev_join, H.lu_small));
     TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
     TABI_CUDA(cudaEventRecord(H.ev_lu_join, H.lu_hi));
@@ -2207,19 +2249,6 @@ void build_precond(Handle& H, cudaStream_t s) {
     }
   }
   lu_phase.reset();
-  // apply lists: blocks of order > 512 get 512 threads (one wave on the GPU),
-  // the others 256 threads on the side stream; largest first in each
-  {
-    std::vector<int> big, small;
-    for (int l = 0; l < nl; ++l) (2 * rng[l].y > 512 ? big : small).push_back(l);
-    std::sort(big.begin(), big.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
-    std::sort(small.begin(), small.end(), [&](int a, int b) { return rng[a].y > rng[b].y; });
-    T.n_solve_big = (int)big.size();
-    T.n_solve_small = (int)small.size();
-    big.insert(big.end(), small.begin(), small.end());
-    H.pc_h_solve_list.assign(big.data(), big.size());
-    H.pc_h_solve_list.upload(T.d_solve_list, s);
-  }
   H.has_precond = true;
 }
 

@@ -89,7 +89,7 @@ struct DBuf {
 // asynchronously.  A copy from pageable memory may wait for the stream's
 // earlier work before it returns, which kept the host from planning while the
 // GPU ran; from page-locked memory the copy returns at once.  `upload`
-// records an event after the copy and `begin` waits for it, so the contents
+// records an event after the copy and `restart` waits for it, so the contents
 // are never rewritten under a pending copy.  Grows only (by doubling, keeping
 // the contents); freeing page-locked memory synchronises the device, so
 // growth should be rare.
@@ -98,10 +98,20 @@ struct PinVec {
   T* p = nullptr;
   size_t len = 0, cap = 0;
   cudaEvent_t done = nullptr;
-  void begin() {
+  // starts a new fill (after the last copy out of the buffer has finished)
+  void restart() {
     if (done) cudaEventSynchronize(done);
     len = 0;
   }
+  // a few std::vector names, for host lists kept on the host as well
+  void clear() { restart(); }
+  void push_back(const T& v) { push(v); }
+  size_t size() const { return len; }
+  bool empty() const { return len == 0; }
+  T* data() { return p; }
+  const T* data() const { return p; }
+  const T* begin() const { return p; }
+  const T* end() const { return p + len; }
   void grow(size_t need) {
     const size_t nc = std::max<size_t>(std::max<size_t>(need, 2 * cap), 256);
     T* q = nullptr;
@@ -116,7 +126,7 @@ struct PinVec {
     p[len++] = v;
   }
   void assign(const T* src, size_t n) {
-    begin();
+    restart();
     if (n > cap) grow(n);
     if (n) std::memcpy(p, src, n * sizeof(T));
     len = n;
@@ -186,7 +196,7 @@ struct Tree {
   DBuf<int64_t> d_slot_off;    // n+1
   DBuf<int2> d_far_ent;        // (target, slot) grouped by cluster
   DBuf<int2> d_near_ent;       // (target, slot) grouped by leaf
-  std::vector<WorkItem> far_work, near_work;
+  PinVec<WorkItem> far_work, near_work;  // page-locked: uploaded per tree
   DBuf<WorkItem> d_far_work, d_near_work;
   int nmslot = 0;
   std::vector<int> mslot_node;  // node id per moment slot

@@ -698,13 +698,8 @@ void build_lists(Handle& H, cudaStream_t s) {
   for (int k = 0; k < T.nmslot; ++k) msc[k] = make_int2(T.mslot_chunk0[k], T.mslot_nchunk[k]);
   T.d_mslot_chunks.alloc(std::max(T.nmslot, 1));
   T.d_mslot_node.alloc(std::max(T.nmslot, 1));
-  if (!T.far_work.empty())
-    TABI_CUDA(cudaMemcpyAsync(T.d_far_work.p, T.far_work.data(),
-                              sizeof(WorkItem) * T.far_work.size(), cudaMemcpyHostToDevice, s));
-  if (!T.near_work.empty())
-    TABI_CUDA(cudaMemcpyAsync(T.d_near_work.p, T.near_work.data(),
-                              sizeof(WorkItem) * T.near_work.size(), cudaMemcpyHostToDevice,
-                              s));
+  T.far_work.upload(T.d_far_work, s);
+  T.near_work.upload(T.d_near_work, s);
   if (!mch.empty())
     TABI_CUDA(cudaMemcpyAsync(T.d_mchunks.p, mch.data(), sizeof(int4) * mch.size(),
                               cudaMemcpyHostToDevice, s));
