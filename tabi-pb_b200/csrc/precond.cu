@@ -1101,7 +1101,11 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     int src = pm[i];
     xs[i] = (src < n) ? r[ib + src] : r[N + ib + src - n];
   }
-  constexpr int kPF = 2;
+  // L2 prefetch distance in steps: one step ahead measured fastest on the
+  // bench molecule (203 us per apply against 225, 249 and 263 us at two,
+  // three and four), as deeper prefetches of all large blocks at once
+  // compete for DRAM and L2 with the loads the steps wait for
+  constexpr int kPF = 1;
   // L panel of step kp: columns kp.., rows below its diagonal block
   auto pf_lower = [&](int kp) {
     if (kp >= m) return;
