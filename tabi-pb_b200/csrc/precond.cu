@@ -1058,16 +1058,6 @@ __global__ void lu_diaginv_kernel(const int2* __restrict__ blocks,  // (leaf, k0
   for (int i = 0; i < kDB; ++i) Ui[(size_t)lane * kDB + i] = x[i];
 }
 
-// L2 prefetch of a byte range (bulk, no completion to wait for); the range
-// starts 16-byte aligned and is a multiple of 16 bytes long, which holds for
-// every column segment of a factor block (even order, offsets of 32 rows).
-__device__ __forceinline__ void prefetch_l2(const double* p, int ndouble) {
-  if (ndouble > 0)
-    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(p),
-                 "r"((unsigned)ndouble * 8u)
-                 : "memory");
-}
-
 // Forward/back substitution with the factored block (DGETRS 'N') in 32-row
 // steps: gather through the pivot permutation, then per step every warp
 // applies the diagonal block's precomputed inverse to the step's 32 running
@@ -1075,9 +1065,11 @@ __device__ __forceinline__ void prefetch_l2(const double* p, int ndouble) {
 // and updates its rows below (above) with a 32-wide GEMV.  The finalised
 // values go to a second array, so one barrier per step suffices: running
 // values r (xs in the forward sweep, fin in the backward one) and results are
-// never the same words within a step.  The steps form a dependent chain, so
-// each one's column panel and inverse block are prefetched into L2 kPF steps
-// ahead (by warp 1).  Large blocks run with 512 threads; leaf_list selects the
+// never the same words within a step.  No L2 prefetch of the coming steps'
+// panels: with all large blocks prefetching at once, one step ahead measured
+// 203 us per apply of the bench molecule, two 225 us, four 263 us, and none
+// 188 us; the prefetches compete for DRAM and L2 with the loads the steps
+// wait for.  Large blocks run with 512 threads; leaf_list selects the
 // launch's leaves.  Shared memory: 2 m + NT doubles.
 template <int NT>
 __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
@@ -1101,24 +1093,6 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     int src = pm[i];
     xs[i] = (src < n) ? r[ib + src] : r[N + ib + src - n];
   }
-  // L2 prefetch distance in steps: one step ahead measured fastest on the
-  // bench molecule (203 us per apply against 225, 249 and 263 us at two,
-  // three and four), as deeper prefetches of all large blocks at once
-  // compete for DRAM and L2 with the loads the steps wait for
-  constexpr int kPF = 1;
-  // L panel of step kp: columns kp.., rows below its diagonal block
-  auto pf_lower = [&](int kp) {
-    if (kp >= m) return;
-    if (kp + lane < m) prefetch_l2(A + (size_t)(kp + lane) * m + kp + kDB, m - kp - kDB);
-    if (lane == 0) prefetch_l2(Di + (size_t)(kp / kDB) * 2 * kDB * kDB, kDB * kDB);
-  };
-  // U panel of block bp: columns bp*32.., rows above its diagonal block
-  auto pf_upper = [&](int bp) {
-    if (bp < 0) return;
-    const int kp = bp * kDB;
-    if (kp + lane < m) prefetch_l2(A + (size_t)(kp + lane) * m, kp);
-    if (lane == 0) prefetch_l2(Di + (size_t)bp * 2 * kDB * kDB + kDB * kDB, kDB * kDB);
-  };
   // the inverse diagonal block of sweep step t (L blocks 0..nblk-1, then U
   // blocks nblk-1..0), staged into shared memory one step ahead by cp.async
   const int nblk = (m + kDB - 1) / kDB;
@@ -1214,24 +1188,18 @@ __global__ void __launch_bounds__(NT, (NT <= 256 ? 4 : 1)) solve_kernel(
     asm volatile("cp.async.wait_group 0;\n" ::);
     __syncthreads();
   };
-  if (warp == 1)
-    for (int q = 0; q < kPF; ++q) pf_lower(q * kDB);
   stage(0, 0);
   asm volatile("cp.async.wait_group 0;\n" ::);
   __syncthreads();
   // L y = P r: running values in xs, y in fin
   for (int k0 = 0, t = 0; k0 < m; k0 += kDB, ++t) {
     const int nb = min(kDB, m - k0);
-    if (warp == 1) pf_lower(k0 + kPF * kDB);
     step(t, k0, nb, xs, fin, k0 + nb, m);
   }
   // U x = y: running values in fin, x in xs
-  if (warp == 1)
-    for (int q = 0; q < kPF; ++q) pf_upper(nblk - 1 - q);
   for (int b = nblk - 1, t = nblk; b >= 0; --b, ++t) {
     const int k0 = b * kDB;
     const int nb = min(kDB, m - k0);
-    if (warp == 1) pf_upper(b - kPF);
     step(t, k0, nb, fin, xs, 0, k0);
   }
   for (int i = tid; i < n; i += NT) {
