@@ -1713,27 +1713,8 @@ void build_precond(Handle& H, cudaStream_t s) {
     H.pc_h_solve_list.assign(big.data(), big.size());
     H.pc_h_solve_list.upload(T.d_solve_list, s);
   }
-  // Two leaf groups with plans of their own: blocks of order above
-  // kLuSmallBlock and the others, so the many short factorisations of small
-  // leaves run beside the long chain of steps of the large ones instead of
-  // inside its launches.  The unpivoted factorisation runs them on the
-  // handle's LU streams (see below); the pivoted one on the caller's stream
-  // and the side stream, with one fork after the assembly and one join at
-  // the end (fork / join).
-  auto fork = [&](bool split) {
-    if (!split) return;
-    TABI_CUDA(cudaEventRecord(H.ev_fork, s));
-    TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
-  };
-  auto join = [&](bool split) {
-    if (!split) return;
-    TABI_CUDA(cudaEventRecord(H.ev_join, H.side));
-    TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
-  };
   // ---- unpivoted factorisation of every leaf, certified (see lu_np_diag_kernel)
-  std::optional<KScope> lu_phase;
-  lu_phase.emplace(H.prof, K_PHASE_LU, s);
-  std::vector<int> pv_leaves;  // leaves factored with partial pivoting
+  H.pc_lu_phase.emplace(H.prof, K_PHASE_LU, s);
   const bool try_np = (H.prm.flags & TABI_FLAG_PIVOTED_LU) == 0;
   if (try_np) {
     DBuf<int>& d_fail = H.pc_fail;
@@ -1957,6 +1938,41 @@ void build_precond(Handle& H, cudaStream_t s) {
       if (big.at < big.plan.size()) issue_one(big);
       if (small.at < small.plan.size()) issue_one(small);
     }
+  }
+}
+
+void finish_precond(Handle& H, cudaStream_t s) {
+  if (H.prm.iprcd != 1 || H.has_precond) return;
+  Tree& T = H.tree;
+  const int nl = T.nleaf;
+  std::vector<int2> rng(nl);
+  for (int l = 0; l < nl; ++l) {
+    const int c = T.leaves[l];
+    rng[l] = make_int2(T.ibeg[c], T.num[c]);
+  }
+  const double eps = H.prm.eps1 / H.prm.eps0;
+  DBuf<int>& d_info = H.pc_info;
+  const bool try_np = (H.prm.flags & TABI_FLAG_PIVOTED_LU) == 0;
+  // Two leaf groups with plans of their own: blocks of order above
+  // kLuSmallBlock and the others, so the many short factorisations of small
+  // leaves run beside the long chain of steps of the large ones instead of
+  // inside its launches.  The unpivoted factorisation runs them on the
+  // handle's LU streams (see below); the pivoted one on the caller's stream
+  // and the side stream, with one fork after the assembly and one join at
+  // the end (fork / join).
+  auto fork = [&](bool split) {
+    if (!split) return;
+    TABI_CUDA(cudaEventRecord(H.ev_fork, s));
+    TABI_CUDA(cudaStreamWaitEvent(H.side, H.ev_fork, 0));
+  };
+  auto join = [&](bool split) {
+    if (!split) return;
+    TABI_CUDA(cudaEventRecord(H.ev_join, H.side));
+    TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
+  };
+  std::vector<int> pv_leaves;  // leaves factored with partial pivoting
+  if (try_np) {
+    DBuf<int>& d_fail = H.pc_fail;
     TABI_CUDA(cudaEventRecord(H.ev_join, H.lu_small));
     TABI_CUDA(cudaStreamWaitEvent(s, H.ev_join, 0));
     TABI_CUDA(cudaEventRecord(H.ev_lu_join, H.lu_hi));
@@ -2220,7 +2236,7 @@ void build_precond(Handle& H, cudaStream_t s) {
                                            " (coincident faces or non-finite surface data)");
     }
   }
-  lu_phase.reset();
+  H.pc_lu_phase.reset();
   H.has_precond = true;
 }
 

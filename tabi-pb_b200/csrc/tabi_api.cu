@@ -2,6 +2,7 @@
 // staging, and the order of the steps main.f90 performs.
 #include <algorithm>
 #include <chrono>
+#include <functional>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -189,12 +190,24 @@ void require_tree(Handle& H, int n2) {
   TABI_REQUIRE(n2 == 2 * H.n, TABI_ERR_ARG, "vector length must be 2*nface");
 }
 
-// the preconditioner factors with the tree: a tree whose leaf blocks cannot be
-// factored (TABI_ERR_SINGULAR) leaves the handle without a tree
-void precond_or_reset(Handle& H, cudaStream_t s) {
+// After the tree: the leaf factorisation is launched on the handle's LU
+// streams first, then the interaction lists are built on s beside it (their
+// host round trips and kernels overlap the factorisation), then the
+// factorisation is joined and checked.  A tree whose leaf blocks cannot be
+// factored (TABI_ERR_SINGULAR), or any failure on the way, leaves the handle
+// without a tree, after the LU streams have finished what was launched.
+void lists_and_precond(Handle& H, cudaStream_t s, const std::function<void(const char*)>& mark) {
   try {
     build_precond(H, s);
+    build_lists(H, s);
+    H.has_tree = true;
+    mark("lists");
+    finish_precond(H, s);
+    mark("precond");
   } catch (...) {
+    for (cudaStream_t x : {H.lu_hi, H.lu_small, H.aux, H.side, s})
+      if (x) cudaStreamSynchronize(x);
+    H.pc_lu_phase.reset();
     H.has_tree = H.has_precond = false;
     throw;
   }
@@ -202,9 +215,7 @@ void precond_or_reset(Handle& H, cudaStream_t s) {
 
 void do_build(Handle& H, cudaStream_t s) {
   build_tree(H, s);
-  build_lists(H, s);
-  H.has_tree = true;
-  precond_or_reset(H, s);
+  lists_and_precond(H, s, [](const char*) {});
 }
 
 template <typename T>
@@ -262,11 +273,7 @@ void run_molecule(Handle& H, WsNet* ws, const MolDev& m, double* x_dev, double* 
   mark("form_matrix");
   build_tree(H, s);
   mark("tree");
-  build_lists(H, s);
-  H.has_tree = true;
-  mark("lists");
-  precond_or_reset(H, s);
-  mark("precond");
+  lists_and_precond(H, s, mark);
   { TABI_K(K_FORM, s); permute_b_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(H.d_perm.p, nface, b0.p, b.p); }
   DBuf<double>& xl = H.rn_x;
   double* x = x_dev;

@@ -8,6 +8,7 @@
 #include <cstring>
 #include <map>
 #include <mutex>
+#include <optional>
 #include <stdexcept>
 #include <string>
 #include <utility>
@@ -332,6 +333,9 @@ struct Handle {
   // chain) and the small-block group below it, so that the block scheduler
   // gives freed SMs to the chain first.
   cudaStream_t lu_hi = nullptr, lu_small = nullptr, aux = nullptr;
+  // the leaf factorisation's phase timer, from its first launch
+  // (build_precond) to the join of its streams (finish_precond)
+  std::optional<KScope> pc_lu_phase;
   // the exchange of a target-sharded solve (tabi_set_exchange)
   tabi_exchange_fn xchg = nullptr;
   void* xchg_user = nullptr;
@@ -443,7 +447,13 @@ void direct_targets_dev(Handle& H, int nt, const int* targets, const double* x, 
                         cudaStream_t s);
 double asum_dev(Handle& H, const double* x, int n, cudaStream_t s);
 // preconditioner (precond.cu)
+// The leaf-block preconditioner in two halves: build_precond assembles the
+// blocks and launches the factorisation on the handle's LU streams (which
+// only need the tree); finish_precond joins them into s, reads the
+// certificates and factors the failed leaves with partial pivoting.  The
+// interaction lists are built in between, on s, beside the factorisation.
 void build_precond(Handle& H, cudaStream_t s);
+void finish_precond(Handle& H, cudaStream_t s);
 void msolve_dev(Handle& H, const double* r, double* z, cudaStream_t s);
 // output_potential (potential.cu): x in tree order -> x_orig (2 n, original
 // face order) and vert_ptl (2 per vertex), both scaled by 332.0716 * 4 pi
