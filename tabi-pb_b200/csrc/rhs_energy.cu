@@ -19,6 +19,11 @@ namespace tabi {
 namespace {
 
 constexpr int kAtomTile = 256;
+// One thread per face, every atom per thread: 64-thread blocks, so that the
+// few hundred blocks a molecule needs spread evenly over the SMs (with
+// 256-thread blocks the 363 of the benchmark molecule put three on some SMs
+// and two on others, which bounded the launch by the busiest ones).
+constexpr int kFaceThreads = 64;
 
 __device__ __forceinline__ double dot3_rn(const double* a, const double* b) {
   return __dadd_rn(__dadd_rn(__dmul_rn(a[0], b[0]), __dmul_rn(a[1], b[1])), __dmul_rn(a[2], b[2]));
@@ -38,7 +43,7 @@ __device__ __forceinline__ double heron(double aa, double bb, double cc) {
 }
 
 // atoms4: (x, y, z, q) per atom
-__global__ void __launch_bounds__(256) form_matrix_kernel(
+__global__ void __launch_bounds__(kFaceThreads) form_matrix_kernel(
     const double* __restrict__ sptpos, const double* __restrict__ sptnrm,
     const int* __restrict__ nvert, int nface, const double* __restrict__ atoms4, int nchr,
     double eps0, double* __restrict__ ox, double* __restrict__ oy, double* __restrict__ oz,
@@ -100,7 +105,7 @@ __global__ void __launch_bounds__(256) form_matrix_kernel(
 }
 
 // RHS only, surface already loaded (SoA)
-__global__ void __launch_bounds__(256) rhs_kernel(const double* __restrict__ px,
+__global__ void __launch_bounds__(kFaceThreads) rhs_kernel(const double* __restrict__ px,
                                                   const double* __restrict__ py,
                                                   const double* __restrict__ pz,
                                                   const double* __restrict__ nx,
@@ -384,14 +389,14 @@ void launch_form_matrix(Handle& H, int nspt, const double* sptpos, const double*
                         int nface, const int* nvert, int nchr, const double* atoms4,
                         double* d_b, cudaStream_t s) {
   (void)nspt;
-  { TABI_K(K_FORM, s); form_matrix_kernel<<<ceil_div(nface, 256), 256, 0, s>>>(
+  { TABI_K(K_FORM, s); form_matrix_kernel<<<ceil_div(nface, kFaceThreads), kFaceThreads, 0, s>>>(
       sptpos, sptnrm, nvert, nface, atoms4, nchr, H.prm.eps0, H.d_x.p, H.d_y.p, H.d_z.p,
       H.d_nx.p, H.d_ny.p, H.d_nz.p, H.d_area.p, d_b); }
   TABI_CUDA(cudaGetLastError());
 }
 
 void launch_rhs(Handle& H, int nchr, const double* atoms4, double* d_b, cudaStream_t s) {
-  { TABI_K(K_FORM, s); rhs_kernel<<<ceil_div(H.n, 256), 256, 0, s>>>(H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p, H.d_ny.p,
+  { TABI_K(K_FORM, s); rhs_kernel<<<ceil_div(H.n, kFaceThreads), kFaceThreads, 0, s>>>(H.d_x.p, H.d_y.p, H.d_z.p, H.d_nx.p, H.d_ny.p,
                                                 H.d_nz.p, H.n, atoms4, nchr, H.prm.eps0, d_b); }
   TABI_CUDA(cudaGetLastError());
 }
